@@ -1,0 +1,328 @@
+"""Benchmark: SSA reaction events/s (and trajectories/s) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME]
+
+Default workload (the one the headline metric is quoted on that fits one
+GPU): plain cuTauLeaping on the bistable Schlogl model, 262,144
+trajectories, X0=250, eps=0.03, n_c=10, 100-step SSA fallback, t_end=5 with
+200 samples.  A step is one full simulation of that workload (one kernel
+launch).  Events are reaction firings (SSA steps plus the Poisson firings of
+each leap).  At N GPUs every rank simulates its own 262,144 trajectories
+(distinct Philox ids; weak scaling, no data-path collective) and the value
+is all events over the slowest rank's device time.
+
+One JSON line on rank 0.  ``--impl reference`` times the CPU restatement of
+the reference algorithm (the oracle port; the reference itself is PyCUDA
+code that cannot run here) on all host cores over a bounded sample.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+import numpy as np  # noqa: E402
+
+METRIC = 'SSA reaction events/s'
+UNIT = 'events/s'
+
+
+def workloads():
+    from py_stoch_b200 import networks
+    return {
+        'schlogl_tau': dict(
+            model=networks.schlogl(), n=262144, method='tau',
+            desc='plain cuTauLeaping, Schlogl (c1=3e-7,c2=1e-4,c3=1e-3,'
+                 'c4=3.5,A=1e5,B=2e5), X0=250, eps=0.03, n_c=10, 100-step '
+                 'SSA fallback, 262144 trajectories, t_end=5, 200 samples',
+            cpu_pilot=1024),
+        'lv_ssa': dict(
+            model=networks.lotka_volterra(), n=1024, method='direct',
+            desc='plain Gillespie direct method, Lotka-Volterra (k1=10, '
+                 'k2=0.01, k3=10), X0=Y0=1000, 1024 trajectories, t_end=10,'
+                 ' 100 samples, Philox ids 0..1023',
+            cpu_pilot=64),
+    }
+
+
+def measured_peaks():
+    p = os.path.join(HERE, 'MEASURED_PEAKS.json')
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d['hbm_gbs']), 'measured'
+    return 6650.0, 'fallback'
+
+
+class ClockSampler(object):
+    """nvidia-smi sampling of SM clock and throttle reasons while running."""
+
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,'
+         'clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
+         'clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,'
+         'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '--query-gpu=' + self.Q, '--format=csv,noheader,'
+                 'nounits', '-i', str(self.idx), '-lms', '100'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(',')])
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], 0.0, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
+                 'sw_power_cap']
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith('active'):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': mx,
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def cpu_baseline(wl, target_s=12.0, threads=0):
+    """Oracle port on host cores over a bounded sample of the workload."""
+    from oracle import oracle
+    m, meth = wl['model'], 0 if wl['method'] == 'direct' else 1
+    n = wl['cpu_pilot']
+    t0 = time.perf_counter()
+    r = oracle.simulate(m, n, meth, seed=0, threads=threads)
+    dt = time.perf_counter() - t0
+    if dt < target_s / 4:
+        n2 = int(min(wl['n'], max(n, n * target_s / max(dt, 1e-3))))
+        t0 = time.perf_counter()
+        r = oracle.simulate(m, n2, meth, seed=1, threads=threads)
+        dt = time.perf_counter() - t0
+        n = n2
+    ev = float(r['events'].sum())
+    cores = threads if threads > 0 else oracle.max_threads()
+    return {'value': ev / dt, 'unit': UNIT, 'cores': cores, 'kind': 'port',
+            'sample': '%d of %d trajectories of the same workload, %.1f s'
+                      % (n, wl['n'], dt),
+            'trajectories_per_s': n / dt}
+
+
+def run_reference(args, wl):
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return 0
+    from oracle import oracle
+    m, meth = wl['model'], 0 if wl['method'] == 'direct' else 1
+    n = wl['cpu_pilot']
+    # size one step to ~ (a few minutes / steps) of CPU work
+    t0 = time.perf_counter()
+    oracle.simulate(m, n, meth, seed=0)
+    dt = time.perf_counter() - t0
+    per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+    n = int(min(wl['n'], max(n, n * per_step / max(dt, 1e-3))))
+    for w in range(args.warmup):
+        oracle.simulate(m, min(n, 256), meth, seed=1000 + w)
+    tot_ev, tot_t = 0.0, 0.0
+    for s in range(args.steps):
+        t0 = time.perf_counter()
+        r = oracle.simulate(m, n, meth, seed=s)
+        tot_t += time.perf_counter() - t0
+        tot_ev += float(r['events'].sum())
+    val = tot_ev / tot_t
+    cores = oracle.max_threads()
+    line = {'impl': 'reference', 'metric': METRIC, 'value': val, 'unit': UNIT,
+            'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': 1e3 * tot_t / args.steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f32/f64', 'data': 'synthetic',
+            'config': {'workload': wl['desc']},
+            'trajectories_per_s': n * args.steps / tot_t,
+            'cpu_baseline': {'value': val, 'unit': UNIT, 'cores': cores,
+                             'kind': 'port',
+                             'sample': '%d of %d trajectories per step'
+                                       % (n, wl['n'])},
+            'e2e': {'value': val, 'unit': UNIT, 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--workload', default='schlogl_tau')
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    args = ap.parse_args()
+    wl = workloads()[args.workload]
+    if args.impl == 'reference':
+        return run_reference(args, wl)
+
+    import torch
+    import torch.distributed as dist
+
+    from py_stoch_b200 import build as _build
+    from py_stoch_b200.simulator import simulate
+
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl',
+                                timeout=datetime.timedelta(seconds=120))
+    dev = torch.device('cuda', local)
+    torch.cuda.set_device(dev)
+    _build.build()
+    m, n, meth = wl['model'], wl['n'], wl['method']
+    base = rank * n
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    out = {'samples': torch.empty((m.kappa, m.ita, n), dtype=torch.int32,
+                                  device=dev),
+           'status': torch.empty(n, dtype=torch.uint8, device=dev),
+           'events': torch.empty(n, dtype=torch.int64, device=dev)}
+
+    def step(seed):
+        return simulate(m, n, method=meth, seed=seed, traj_id_base=base,
+                        device=dev, stream=stream, out=out)
+
+    for w in range(args.warmup):
+        step(10_000 + w)
+    torch.cuda.synchronize(dev)
+    clk = ClockSampler(local)
+    clk.start()
+    total_ms, events = 0.0, 0
+    errs = 0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    for s in range(args.steps):
+        flush.fill_(s & 0xFF)
+        st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(
+            enable_timing=True)
+        st.record(stream)
+        res = step(s)
+        en.record(stream)
+        en.synchronize()
+        total_ms += st.elapsed_time(en)
+        events += int(res['events'].sum().item())
+        errs += int((res['status'] >= 2).sum().item())
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = clk.stop()
+    t = torch.tensor([total_ms, float(events), float(errs)], dtype=torch.float64,
+                     device=dev)
+    if world > 1:
+        tm = t[:1].clone()
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        t[0] = tm[0]
+    total_ms, events, errs = float(t[0]), float(t[1]), float(t[2])
+    sec = total_ms / 1e3
+    value = events / sec
+
+    # end to end through the public API: pinned host model blob in, samples
+    # and per-trajectory status/events out, every step
+    blob = torch.from_numpy(m.blob().view(np.int32)).pin_memory()
+    d_blob = torch.empty_like(blob, device=dev)
+    h_out = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+             for k, v in out.items()}
+    e2e_ms, e2e_ev = 0.0, 0
+    for s in range(args.steps):
+        flush.fill_(s & 0xFF)
+        st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(
+            enable_timing=True)
+        st.record(stream)
+        d_blob.copy_(blob, non_blocking=True)
+        res = simulate(m, n, method=meth, seed=100 + s, traj_id_base=base,
+                       device=dev, stream=stream, out=out, d_blob=d_blob)
+        for k in h_out:
+            h_out[k].copy_(out[k], non_blocking=True)
+        en.record(stream)
+        en.synchronize()
+        e2e_ms += st.elapsed_time(en)
+        e2e_ev += int(h_out['events'].sum())
+    e2 = torch.tensor([e2e_ms, float(e2e_ev)], dtype=torch.float64, device=dev)
+    if world > 1:
+        tm = e2[:1].clone()
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        dist.all_reduce(e2, op=dist.ReduceOp.SUM)
+        e2[0] = tm[0]
+    e2e_value = float(e2[1]) / (float(e2[0]) / 1e3)
+    h2d = blob.numel() * 4
+    d2h = sum(v.numel() * v.element_size() for v in h_out.values())
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        out_bytes = sum(v.numel() * v.element_size() for v in out.values())
+        per_launch_s = sec / args.steps / 1.0
+        achieved = out_bytes / per_launch_s / 1e9
+        line = {
+            'metric': METRIC, 'value': value, 'unit': UNIT,
+            'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': total_ms / args.steps, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32/f64',
+            'data': 'synthetic',
+            'config': {'workload': wl['desc'], 'trajectories_per_gpu': n,
+                       'l2': 'flushed (256 MiB write) before every step',
+                       'parallelism': 'trajectory shards, one per GPU'},
+            'trajectories_per_s': n * world * args.steps / sec,
+            'events_per_step': events / args.steps,
+            'error_trajectories': int(errs),
+            'gpu_launches': args.steps,
+            'e2e': {'value': e2e_value, 'unit': UNIT,
+                    'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h},
+            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak,
+                         'unit': 'GB/s', 'frac': achieved / peak,
+                         'traffic': None, 'peak_source': peak_kind,
+                         'note': 'the kernel is CUDA-core issue bound; HBM '
+                                 'carries only the sample output'},
+            'clocks': clocks,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line['cpu_baseline'] = cpu_baseline(wl)
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == '__main__':
+    sys.exit(main())

@@ -1,0 +1,253 @@
+/*
+ * pystoch_b200.h -- C ABI of the B200 stochastic-simulation engine.
+ *
+ * The engine replaces the simulator layer of py_stoch (reference paths
+ * below are relative to the reference project).  Every entry point takes
+ * plain pointers and sizes; device pointers must be CUDA device memory
+ * owned by the caller, and `stream` is a cudaStream_t passed as void*.
+ * The library allocates no device memory on any entry point: scratch is
+ * caller-provided workspace whose size the *_workspace_size functions
+ * return.  Calls are stream-ordered and return before the GPU finishes.
+ *
+ * Replaces:
+ *   CuGillespie.run        mod/simulator/cuGillespie/cuGillespie.py:16-46
+ *                          (kernel_Gillespie, gillespie.py:27-149)
+ *   CuTauLeaping.run       mod/simulator/cuTauLeaping/cuTauLeaping.py:18-84
+ *                          (kernel_P1_P2, P1_P2.py:54-297;
+ *                           kernel_P3, P3.py:29-163;
+ *                           termination sum, cuTauLeaping.py:72)
+ *   init_rng               mod/simulator/simulator.py:62-96
+ *                          (replaced by the stateless Philox4x32-10 stream)
+ *   __constant__ uploads   cuTauLeaping.py:86-107, cuGillespie.py:49-63
+ *                          (replaced by the model blob, pyst_model_build)
+ *   calculate_sizes        simulator.py:11-58, cuTauLeaping.py:162-214
+ *                          (launch geometry is chosen inside the library)
+ */
+#ifndef PYSTOCH_B200_H
+#define PYSTOCH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PYST_ABI_VERSION 1
+
+/* ---- return codes ------------------------------------------------------ */
+enum {
+  PYST_OK = 0,
+  PYST_EINVAL = 1,        /* bad argument (null pointer, size, alignment)   */
+  PYST_ECUDA = 2,         /* a CUDA runtime call failed                     */
+  PYST_EUNSUPPORTED = 3,  /* model exceeds a kernel limit (see below)       */
+  PYST_EWORKSPACE = 4,    /* workspace smaller than *_workspace_size        */
+  PYST_ETRAJ = 5          /* some trajectory ended with an error status     */
+};
+
+/* ---- per-trajectory status (uint8 array written by the run calls) ----- */
+enum {
+  PYST_TRAJ_DONE = 0,         /* reached the last sample time              */
+  PYST_TRAJ_ABSORBED = 1,     /* total propensity hit 0; samples filled    */
+  PYST_TRAJ_STEP_BUDGET = 2,  /* step budget exhausted; rest filled -1     */
+  PYST_TRAJ_OVERFLOW = 3,     /* a species count would leave int32 range   */
+  PYST_TRAJ_LEAP_RETRY = 4,   /* tau halved max_leap_retries times         */
+  PYST_TRAJ_SAMPLER = 5,      /* Poisson sampler hit its iteration limit   */
+  PYST_TRAJ_STAGING = 6       /* model staging into shared memory timed out */
+};
+
+/* ---- methods and mappings ---------------------------------------------- */
+enum { PYST_METHOD_DIRECT = 0, PYST_METHOD_TAU_LEAP = 1 };
+enum { PYST_MAP_AUTO = 0, PYST_MAP_THREAD = 1, PYST_MAP_WARP = 2 };
+
+/* Limits of this build. */
+#define PYST_MAX_SPECIES 1024
+#define PYST_MAX_REACTIONS 4096
+#define PYST_THREAD_MAX_REACTIONS 32  /* thread-per-trajectory kernels      */
+#define PYST_MAX_BLOB_WORDS 12288     /* model blob staged in 48 KiB smem   */
+
+/*
+ * Mass-action model description (host pointers).  Matrices are dense,
+ * row-major [species][reaction], the layout of SPN.Pre / SPN.Post
+ * (mod/petri_net/SPN.py:72-97).
+ *
+ * Propensity of reaction j:
+ *   a_j(x) = rate[j] * prod_i prod_{m < order[i][j]} (x_i - m * falling[i][j])
+ * computed in FP32 in species order, factors in m order.
+ */
+typedef struct pyst_model_desc {
+  int32_t n_species;           /* S = TlArgs.N                              */
+  int32_t n_reactions;         /* R = TlArgs.M                              */
+  const int32_t* order;        /* [S*R] propensity order per species        */
+  const uint8_t* falling;      /* [S*R] 1 falling factorial, 0 power; NULL=1 */
+  const int32_t* pre;          /* [S*R] SPN.Pre (reactant species set)      */
+  const int32_t* net_change;   /* [S*R] SPN.Post - SPN.Pre (TlArgs.V dense) */
+  const double* rate;          /* [R] effective rate constants              */
+  const int32_t* x0;           /* [S] TlArgs.x_0                            */
+  const int32_t* hor;          /* [S] TlArgs.H                              */
+  const int32_t* hor_type;     /* [S] TlArgs.H_type                         */
+  const float* sample_times;   /* [ita] TlArgs.I (float32, ascending)       */
+  int32_t n_samples;           /* ita                                       */
+  const int32_t* out_species;  /* [kappa] TlArgs.E                          */
+  int32_t n_out;               /* kappa                                     */
+  double t_max;                /* TlArgs.t_max                              */
+  float eta;                   /* TlArgs.eta (0.03)                         */
+  int32_t n_c;                 /* TlArgs.n_c (10)                           */
+} pyst_model_desc;
+
+/* Run description.  Trajectory u (0 <= u < n_traj) draws from the Philox
+ * stream keyed by `seed` with counter words (block index, block index >> 32,
+ * id, id >> 32) where id = traj_id_base + u. */
+typedef struct pyst_run_desc {
+  int64_t n_traj;              /* U                                         */
+  int64_t traj_id_base;        /* global id of trajectory 0                 */
+  uint64_t seed;               /* Philox key                                */
+  int32_t method;              /* PYST_METHOD_*                             */
+  int32_t mapping;             /* PYST_MAP_*                                */
+  int32_t ssa_fallback_steps;  /* SSA steps per fallback round (100)        */
+  int32_t max_leap_retries;    /* tau halvings before giving up (64)        */
+  int64_t step_budget;         /* max steps per trajectory (0 = 2^62)       */
+  int32_t block_size;          /* 0 = library default                       */
+  int32_t flags;               /* reserved, 0                               */
+} pyst_run_desc;
+
+/* Outputs (device pointers).  `samples` is required, the rest optional. */
+typedef struct pyst_outputs {
+  int32_t* samples;   /* [kappa][ita][out_stride], trajectory innermost     */
+  int64_t out_stride; /* >= n_traj; 0 means n_traj                          */
+  uint8_t* status;    /* [n_traj] PYST_TRAJ_*                               */
+  int64_t* events;    /* [n_traj] reaction firings                          */
+  uint64_t* seqhash;  /* [n_traj] FNV-1a hash of the firing sequence        */
+  double* t_final;    /* [n_traj] clock when the trajectory stopped         */
+  double* score;      /* [n_traj][R] d log p / d log rate_j                 */
+} pyst_outputs;
+
+/* ---- model blob (host side, no CUDA) ----------------------------------- */
+
+/* Number of 32-bit words of the packed model (a multiple of 4). */
+int pyst_model_blob_words(const pyst_model_desc* model, int64_t* n_words);
+
+/* Pack `model` into `blob` (host memory, n_words words).  The caller copies
+ * the blob to 16-byte-aligned device memory for the run calls. */
+int pyst_model_build(const pyst_model_desc* model, uint32_t* blob,
+                     int64_t n_words);
+
+/* ---- single-model runs -------------------------------------------------- */
+
+/* Both single-model runs take the blob twice: `h_blob` (host copy; only
+ * its header is read, to size the launch without a device round trip) and
+ * `d_blob` (16-byte-aligned device copy the kernels stage). */
+
+/* Direct-method SSA (Gillespie), one trajectory per thread or per warp.
+ * Replaces CuGillespie.run and the forced-SSA path of CuTauLeaping.run
+ * (gillespie=1, P1_P2.py:68-74 + P3.py:71-151). */
+int pyst_ssa_direct_run(const uint32_t* h_blob, const uint32_t* d_blob,
+                        const pyst_run_desc* run, const pyst_outputs* out,
+                        void* stream);
+
+/* Adaptive tau-leaping with critical reactions and SSA fallback, all
+ * rounds inside one launch.  Replaces CuTauLeaping.run (host round loop
+ * cuTauLeaping.py:49-76 with kernel_P1_P2 and kernel_P3). */
+int pyst_tau_leap_run(const uint32_t* h_blob, const uint32_t* d_blob,
+                      const pyst_run_desc* run, const pyst_outputs* out,
+                      void* stream);
+
+/* ---- batched persistent runs -------------------------------------------- */
+
+/* One work item: a model, its trajectories and where its outputs go.
+ * Offsets are in elements of the corresponding output arrays; an item's
+ * samples are [kappa][ita][n_traj] starting at sample_offset. */
+typedef struct pyst_batch_item {
+  int64_t blob_offset;     /* word offset of the model blob in d_blobs     */
+  int64_t n_traj;          /* trajectories of this item                    */
+  int64_t traj_id_base;    /* Philox id of its trajectory 0                */
+  int64_t sample_offset;   /* element offset of its [kappa][ita][n_traj]   */
+  int64_t traj_offset;     /* element offset into status/events/... arrays */
+  int64_t score_offset;    /* element offset into score ([n_traj][R])      */
+  int32_t method;          /* PYST_METHOD_*                                */
+  int32_t mapping;         /* PYST_MAP_THREAD or PYST_MAP_WARP             */
+} pyst_batch_item;
+
+/* Largest model of a batch (sizes the shared-memory layout). */
+typedef struct pyst_batch_limits {
+  int32_t max_blob_words;
+  int32_t max_species;
+  int32_t max_reactions;
+  int32_t reserved;
+} pyst_batch_limits;
+
+/* Workspace bytes pyst_batch_run needs for n_items items. */
+int pyst_batch_workspace_size(int64_t n_items, size_t* bytes);
+
+/* Run every item in one persistent launch.  `d_items` is device memory
+ * holding n_items pyst_batch_item; blocks take items from a device work
+ * queue in array order (put expensive items first).  Per-trajectory output
+ * pointers in `out` are bases that the item offsets index.  The run fields
+ * n_traj, traj_id_base, method and mapping are taken from the items. */
+int pyst_batch_run(const uint32_t* d_blobs, const pyst_batch_item* d_items,
+                   int64_t n_items, const pyst_batch_limits* limits,
+                   const pyst_run_desc* run, const pyst_outputs* out,
+                   void* d_workspace, size_t workspace_bytes, void* stream);
+
+/* ---- likelihood-ratio gradient ------------------------------------------ */
+
+/* grad[j] = (1/U) sum_u h_u * score[u][j] with
+ *   h_u = sum_{k,f} gmean[k][f] (O[k][f][u] - mean[k][f])
+ *                 + gvar[k][f] ((O[k][f][u] - mean[k][f])^2 - var[k][f]).
+ * `samples` is [kappa][ita][U] int32, `score` [U][R] double; mean, var,
+ * gmean, gvar are [kappa][ita] double (gvar may be NULL).  Writes R doubles
+ * to d_grad.  Deterministic: fixed reduction order for a given U. */
+int pyst_score_backward_workspace_size(int64_t n_traj, int32_t n_reactions,
+                                       size_t* bytes);
+int pyst_score_backward(const int32_t* samples, const double* score,
+                        int64_t n_traj, int32_t kappa, int32_t ita,
+                        int32_t n_reactions, const double* mean,
+                        const double* var, const double* gmean,
+                        const double* gvar, double* d_grad,
+                        void* d_workspace, size_t workspace_bytes,
+                        void* stream);
+
+/* ---- misc -------------------------------------------------------------- */
+
+int pyst_abi_version(void);
+const char* pyst_status_string(int code);
+const char* pyst_traj_status_string(int code);
+
+/* Blob header layout (word indices), shared by the packer and kernels. */
+enum {
+  PYST_H_MAGIC = 0,      /* 0x31545950 */
+  PYST_H_WORDS = 1,
+  PYST_H_S = 2,
+  PYST_H_R = 3,
+  PYST_H_KAPPA = 4,
+  PYST_H_ITA = 5,
+  PYST_H_NFAC = 6,
+  PYST_H_NNET = 7,
+  PYST_H_NSPV = 8,
+  PYST_H_NCRIT = 9,
+  PYST_H_OFF_RATE = 10,     /* f32[R]                                       */
+  PYST_H_OFF_FACPTR = 11,   /* i32[R+1]                                     */
+  PYST_H_OFF_FAC = 12,      /* species | order<<16 | falling<<24            */
+  PYST_H_OFF_NETPTR = 13,   /* i32[R+1]                                     */
+  PYST_H_OFF_NET = 14,      /* species | (int16 delta)<<16                  */
+  PYST_H_OFF_TIMES = 15,    /* f32[ita]                                     */
+  PYST_H_OFF_OUT = 16,      /* i32[kappa]                                   */
+  PYST_H_OFF_X0 = 17,       /* i32[S]                                       */
+  PYST_H_OFF_SPVPTR = 18,   /* i32[S+1] species-major V of reactant species */
+  PYST_H_OFF_SPV = 19,      /* reaction | (int16 v)<<16                     */
+  PYST_H_OFF_G = 20,        /* H | H_type<<8 | reactant<<16                 */
+  PYST_H_OFF_CRITPTR = 21,  /* i32[R+1]                                     */
+  PYST_H_OFF_CRIT = 22,     /* species | |v|<<16 (entries with v < 0)       */
+  PYST_H_NC = 23,
+  PYST_H_ETA = 24,          /* f32 bits                                     */
+  PYST_H_FLAGS = 25,
+  PYST_H_TMAX_LO = 26,      /* f64 bits                                     */
+  PYST_H_TMAX_HI = 27,
+  PYST_H_WORDS_HEADER = 32
+};
+#define PYST_BLOB_MAGIC 0x31545950u
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,192 @@
+"""Batched persistent runs: many models of uneven size in one launch.
+
+The reference runs a sweep as one JIT compile and one host-driven launch
+sequence per parameter combination (``examples/schlogl_sim.py:66-80``,
+``examples/PL_sim.py:73-89``).  :class:`Batch` packs every model into one
+device blob table and one item table, allocates all outputs once, and runs
+everything with a single ``pyst_batch_run`` launch whose blocks pull items
+from a device work queue (largest estimated cost first).
+
+Outputs of item ``i`` are views: ``batch.samples(i)`` is
+``[kappa_i, ita_i, n_traj_i]``; per-trajectory arrays are sliced the same
+way.
+"""
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .simulator import _mapping, _method, _torch
+
+
+def estimated_cost(model, method):
+    """Rough work estimate of one trajectory: total propensity at x0 times
+    the simulated time (events for the direct method)."""
+    x = model.x0.astype(np.float64)
+    a0 = 0.0
+    for j in range(model.n_reactions):
+        a = float(model.rate[j])
+        for i in range(model.n_species):
+            n = int(model.order[i, j])
+            for q in range(n):
+                a *= max(x[i] - q * int(model.falling[i, j]), 0.0)
+        a0 += a
+    cost = max(a0, 1.0) * float(model.sample_times[-1])
+    if _method(method) == _lib.METHOD_TAU_LEAP:
+        cost = min(cost, 1e4 * float(model.sample_times[-1]) + 1.0)
+    return cost * (1.0 + model.n_reactions / 32.0)
+
+
+def auto_mapping(model):
+    if (model.n_reactions <= _lib.THREAD_MAX_REACTIONS
+            and model.n_species <= 64):
+        return _lib.MAP_THREAD
+    return _lib.MAP_WARP
+
+
+class Batch(object):
+    """A set of (model, trajectories, method, mapping) items."""
+
+    def __init__(self, models, n_traj, method='direct', mapping='auto',
+                 traj_id_base=None, device=None, score=False, status=True,
+                 events=True, seqhash=False, t_final=False, order='cost',
+                 mapping_fn=None):
+        torch = _torch()
+        self.device = torch.device(device or 'cuda')
+        self.models = list(models)
+        n = len(self.models)
+        self.n_traj = (np.full(n, int(n_traj), np.int64)
+                       if np.isscalar(n_traj) else
+                       np.asarray(n_traj, np.int64))
+        meths = ([method] * n if isinstance(method, (str, int)) else
+                 list(method))
+        self.methods = np.array([_method(m) for m in meths], np.int32)
+        if mapping_fn is not None:
+            maps = [mapping_fn(m, me) for m, me in zip(self.models,
+                                                       self.methods)]
+        elif isinstance(mapping, (str, int)):
+            maps = [mapping] * n
+        else:
+            maps = list(mapping)
+        mp = []
+        for m, x in zip(self.models, maps):
+            x = _mapping(x)
+            if x == _lib.MAP_AUTO:
+                x = auto_mapping(m)
+            if x == _lib.MAP_THREAD and (
+                    m.n_reactions > _lib.THREAD_MAX_REACTIONS):
+                x = _lib.MAP_WARP
+            mp.append(x)
+        self.mappings = np.array(mp, np.int32)
+        if traj_id_base is None:
+            traj_id_base = np.concatenate([[0], np.cumsum(self.n_traj)[:-1]])
+        self.traj_id_base = np.asarray(traj_id_base, np.int64)
+
+        blobs = [m.blob() for m in self.models]
+        self.blob_offset = np.concatenate(
+            [[0], np.cumsum([len(b) for b in blobs])[:-1]]).astype(np.int64)
+        self.kappa = np.array([m.kappa for m in self.models], np.int64)
+        self.ita = np.array([m.ita for m in self.models], np.int64)
+        self.R = np.array([m.n_reactions for m in self.models], np.int64)
+        sizes = self.kappa * self.ita * self.n_traj
+        self.sample_offset = np.concatenate(
+            [[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+        self.traj_offset = np.concatenate(
+            [[0], np.cumsum(self.n_traj)[:-1]]).astype(np.int64)
+        self.score_offset = np.concatenate(
+            [[0], np.cumsum(self.n_traj * self.R)[:-1]]).astype(np.int64)
+        self.total_traj = int(self.n_traj.sum())
+
+        if order == 'cost':
+            cost = np.array([estimated_cost(m, me) * nt for m, me, nt in
+                             zip(self.models, self.methods, self.n_traj)])
+            self.run_order = np.argsort(-cost, kind='stable')
+        else:
+            self.run_order = np.arange(n)
+        items = (_lib.BatchItem * n)()
+        for slot, i in enumerate(self.run_order):
+            it = items[slot]
+            it.blob_offset = int(self.blob_offset[i])
+            it.n_traj = int(self.n_traj[i])
+            it.traj_id_base = int(self.traj_id_base[i])
+            it.sample_offset = int(self.sample_offset[i])
+            it.traj_offset = int(self.traj_offset[i])
+            it.score_offset = int(self.score_offset[i])
+            it.method = int(self.methods[i])
+            it.mapping = int(self.mappings[i])
+        raw = np.frombuffer(bytes(items), dtype=np.uint8)
+        self.d_items = torch.from_numpy(raw.copy()).to(self.device)
+        self.d_blobs = torch.from_numpy(
+            np.concatenate(blobs).view(np.int32)).to(self.device)
+        self.limits = _lib.BatchLimits(
+            max(len(b) for b in blobs),
+            max(m.n_species for m in self.models),
+            max(m.n_reactions for m in self.models), 0)
+        L = _lib.lib()
+        ws = C.c_size_t(0)
+        _lib.check(L.pyst_batch_workspace_size(n, C.byref(ws)),
+                   'pyst_batch_workspace_size')
+        self.workspace = torch.empty(int(ws.value), dtype=torch.uint8,
+                                     device=self.device)
+        dev = self.device
+        self.out = {'samples': torch.empty(int(sizes.sum()),
+                                           dtype=torch.int32, device=dev)}
+        if status:
+            self.out['status'] = torch.empty(self.total_traj,
+                                             dtype=torch.uint8, device=dev)
+        if events:
+            self.out['events'] = torch.empty(self.total_traj,
+                                             dtype=torch.int64, device=dev)
+        if seqhash:
+            self.out['seqhash'] = torch.empty(self.total_traj,
+                                              dtype=torch.int64, device=dev)
+        if t_final:
+            self.out['t_final'] = torch.empty(self.total_traj,
+                                              dtype=torch.float64, device=dev)
+        if score:
+            self.out['score'] = torch.empty(int((self.n_traj * self.R).sum()),
+                                            dtype=torch.float64, device=dev)
+
+    def run(self, seed=0, stream=None, ssa_fallback_steps=100,
+            max_leap_retries=63, step_budget=0, block_size=0):
+        """Enqueue the whole batch on ``stream`` (one kernel launch)."""
+        torch = _torch()
+        L = _lib.lib()
+        o = self.out
+        outs = _lib.Outputs(
+            o['samples'].data_ptr(), 0,
+            o['status'].data_ptr() if 'status' in o else 0,
+            o['events'].data_ptr() if 'events' in o else 0,
+            o['seqhash'].data_ptr() if 'seqhash' in o else 0,
+            o['t_final'].data_ptr() if 't_final' in o else 0,
+            o['score'].data_ptr() if 'score' in o else 0)
+        r = _lib.RunDesc(0, 0, int(seed) & 0xFFFFFFFFFFFFFFFF, 0, 0,
+                         int(ssa_fallback_steps), int(max_leap_retries),
+                         int(step_budget), int(block_size), 0)
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        _lib.check(L.pyst_batch_run(
+            self.d_blobs.data_ptr(), self.d_items.data_ptr(),
+            len(self.models), C.byref(self.limits), C.byref(r),
+            C.byref(outs), self.workspace.data_ptr(),
+            self.workspace.numel(), C.c_void_p(stream.cuda_stream)),
+            'pyst_batch_run')
+        return self
+
+    # ---- per-item views -------------------------------------------------
+    def samples(self, i):
+        a = int(self.sample_offset[i])
+        n = int(self.kappa[i] * self.ita[i] * self.n_traj[i])
+        return self.out['samples'][a:a + n].view(
+            int(self.kappa[i]), int(self.ita[i]), int(self.n_traj[i]))
+
+    def per_traj(self, name, i):
+        a = int(self.traj_offset[i])
+        return self.out[name][a:a + int(self.n_traj[i])]
+
+    def score(self, i):
+        a = int(self.score_offset[i])
+        n = int(self.n_traj[i] * self.R[i])
+        return self.out['score'][a:a + n].view(int(self.n_traj[i]),
+                                               int(self.R[i]))

@@ -1,0 +1,243 @@
+// C ABI of libpystoch_b200.so (include/pystoch_b200.h): argument checks,
+// launch-geometry choice and dispatch to the kernel translation units.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+
+#include "pyst_launch.cuh"
+#include "pystoch_b200.h"
+
+namespace pyst {
+
+int num_sms() {
+  static std::atomic<int> cached{0};
+  int n = cached.load();
+  if (n) return n;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) !=
+          cudaSuccess ||
+      n <= 0)
+    return 148;
+  cached.store(n);
+  return n;
+}
+
+}  // namespace pyst
+
+using namespace pyst;
+
+namespace {
+
+int read_header(const uint32_t* h, HostModelInfo* mi) {
+  if (!h) return PYST_EINVAL;
+  if (h[PYST_H_MAGIC] != PYST_BLOB_MAGIC) return PYST_EINVAL;
+  mi->words = (int)h[PYST_H_WORDS];
+  mi->S = (int)h[PYST_H_S];
+  mi->R = (int)h[PYST_H_R];
+  if (mi->words <= 0 || (mi->words & 3) || mi->words > PYST_MAX_BLOB_WORDS)
+    return PYST_EUNSUPPORTED;
+  if (mi->S < 1 || mi->R < 1 || mi->S > PYST_MAX_SPECIES ||
+      mi->R > PYST_MAX_REACTIONS)
+    return PYST_EUNSUPPORTED;
+  return PYST_OK;
+}
+
+int check_run(const pyst_run_desc* run) {
+  if (!run) return PYST_EINVAL;
+  if (run->n_traj < 0 || run->traj_id_base < 0) return PYST_EINVAL;
+  if (run->method != PYST_METHOD_DIRECT && run->method != PYST_METHOD_TAU_LEAP)
+    return PYST_EINVAL;
+  if (run->mapping < PYST_MAP_AUTO || run->mapping > PYST_MAP_WARP)
+    return PYST_EINVAL;
+  if (run->method == PYST_METHOD_TAU_LEAP &&
+      (run->ssa_fallback_steps < 1 || run->max_leap_retries < 0 ||
+       run->max_leap_retries > 63))
+    return PYST_EINVAL;
+  if (run->step_budget < 0) return PYST_EINVAL;
+  if (run->block_size != 0 &&
+      (run->block_size < 32 || run->block_size > 128 || run->block_size % 32))
+    return PYST_EINVAL;
+  return PYST_OK;
+}
+
+RunArgs make_args(const pyst_run_desc* run) {
+  RunArgs ra;
+  ra.seed = run->seed;
+  ra.step_budget = run->step_budget ? run->step_budget : (1ll << 62);
+  ra.ssa_fallback_steps =
+      run->ssa_fallback_steps > 0 ? run->ssa_fallback_steps : 100;
+  ra.max_leap_retries = run->max_leap_retries;
+  return ra;
+}
+
+OutBase make_outbase(const pyst_outputs* out, int64_t n_traj) {
+  OutBase ob;
+  ob.samples = out->samples;
+  ob.stride = out->out_stride ? out->out_stride : n_traj;
+  ob.status = out->status;
+  ob.events = out->events;
+  ob.seqhash = out->seqhash;
+  ob.t_final = out->t_final;
+  ob.score = out->score;
+  return ob;
+}
+
+int single_run(const uint32_t* h_blob, const uint32_t* d_blob,
+               const pyst_run_desc* run, const pyst_outputs* out, void* stream,
+               int method) {
+  HostModelInfo mi;
+  int rc = read_header(h_blob, &mi);
+  if (rc) return rc;
+  rc = check_run(run);
+  if (rc) return rc;
+  if (run->method != method) return PYST_EINVAL;
+  if (!d_blob || ((uintptr_t)d_blob & 15)) return PYST_EINVAL;
+  if (!out || !out->samples) return PYST_EINVAL;
+  if (out->out_stride != 0 && out->out_stride < run->n_traj)
+    return PYST_EINVAL;
+  if (run->n_traj == 0) return PYST_OK;
+  const RunArgs ra = make_args(run);
+  const OutBase ob = make_outbase(out, run->n_traj);
+  cudaStream_t st = (cudaStream_t)stream;
+  const bool tau = method == PYST_METHOD_TAU_LEAP;
+  const bool score = out->score != nullptr;
+  int mapping = run->mapping;
+  const int bs = run->block_size ? run->block_size : 128;
+  if (mapping == PYST_MAP_AUTO)
+    mapping = (mi.R <= PYST_THREAD_MAX_REACTIONS && mi.S <= 64)
+                  ? PYST_MAP_THREAD
+                  : PYST_MAP_WARP;
+  if (mapping == PYST_MAP_THREAD && mi.R > PYST_THREAD_MAX_REACTIONS)
+    return PYST_EUNSUPPORTED;
+  const uint64_t idb = (uint64_t)run->traj_id_base;
+  const int64_t n = run->n_traj;
+  if (mapping == PYST_MAP_THREAD) {
+    if (tau)
+      return score ? launch_plain_thread_11(mi.R, d_blob, mi, n, idb, ra, ob,
+                                            bs, st)
+                   : launch_plain_thread_10(mi.R, d_blob, mi, n, idb, ra, ob,
+                                            bs, st);
+    return score ? launch_plain_thread_01(mi.R, d_blob, mi, n, idb, ra, ob, bs,
+                                          st)
+                 : launch_plain_thread_00(mi.R, d_blob, mi, n, idb, ra, ob, bs,
+                                          st);
+  }
+  if (tau)
+    return score ? launch_plain_warp_11(d_blob, mi, n, idb, ra, ob, bs, st)
+                 : launch_plain_warp_10(d_blob, mi, n, idb, ra, ob, bs, st);
+  return score ? launch_plain_warp_01(d_blob, mi, n, idb, ra, ob, bs, st)
+               : launch_plain_warp_00(d_blob, mi, n, idb, ra, ob, bs, st);
+}
+
+}  // namespace
+
+extern "C" {
+
+int pyst_abi_version(void) { return PYST_ABI_VERSION; }
+
+const char* pyst_status_string(int code) {
+  switch (code) {
+    case PYST_OK: return "ok";
+    case PYST_EINVAL: return "invalid argument";
+    case PYST_ECUDA: return "CUDA runtime error";
+    case PYST_EUNSUPPORTED: return "model exceeds a kernel limit";
+    case PYST_EWORKSPACE: return "workspace too small";
+    case PYST_ETRAJ: return "a trajectory ended with an error status";
+  }
+  return "unknown status";
+}
+
+const char* pyst_traj_status_string(int code) {
+  switch (code) {
+    case PYST_TRAJ_DONE: return "done";
+    case PYST_TRAJ_ABSORBED: return "absorbed (total propensity 0)";
+    case PYST_TRAJ_STEP_BUDGET: return "step budget exhausted";
+    case PYST_TRAJ_OVERFLOW: return "species count out of int32 range";
+    case PYST_TRAJ_LEAP_RETRY: return "tau halved too many times";
+    case PYST_TRAJ_SAMPLER: return "Poisson sampler iteration limit";
+    case PYST_TRAJ_STAGING: return "model staging timed out";
+  }
+  return "unknown trajectory status";
+}
+
+int pyst_ssa_direct_run(const uint32_t* h_blob, const uint32_t* d_blob,
+                        const pyst_run_desc* run, const pyst_outputs* out,
+                        void* stream) {
+  return single_run(h_blob, d_blob, run, out, stream, PYST_METHOD_DIRECT);
+}
+
+int pyst_tau_leap_run(const uint32_t* h_blob, const uint32_t* d_blob,
+                      const pyst_run_desc* run, const pyst_outputs* out,
+                      void* stream) {
+  return single_run(h_blob, d_blob, run, out, stream, PYST_METHOD_TAU_LEAP);
+}
+
+int pyst_batch_workspace_size(int64_t n_items, size_t* bytes) {
+  if (!bytes || n_items < 0) return PYST_EINVAL;
+  *bytes = 256;  // the work-queue counter, padded
+  return PYST_OK;
+}
+
+int pyst_batch_run(const uint32_t* d_blobs, const pyst_batch_item* d_items,
+                   int64_t n_items, const pyst_batch_limits* lim,
+                   const pyst_run_desc* run, const pyst_outputs* out,
+                   void* d_workspace, size_t workspace_bytes, void* stream) {
+  if (!d_blobs || !d_items || !lim || !run || !out || !out->samples)
+    return PYST_EINVAL;
+  if (((uintptr_t)d_blobs & 15) || n_items < 0) return PYST_EINVAL;
+  if (!d_workspace || ((uintptr_t)d_workspace & 7)) return PYST_EINVAL;
+  if (workspace_bytes < 256) return PYST_EWORKSPACE;
+  if (lim->max_blob_words <= 0 || (lim->max_blob_words & 3) ||
+      lim->max_blob_words > PYST_MAX_BLOB_WORDS || lim->max_species < 1 ||
+      lim->max_reactions < 1 || lim->max_species > PYST_MAX_SPECIES ||
+      lim->max_reactions > PYST_MAX_REACTIONS)
+    return PYST_EUNSUPPORTED;
+  if (run->step_budget < 0 || run->ssa_fallback_steps < 1 ||
+      run->max_leap_retries < 0 || run->max_leap_retries > 63)
+    return PYST_EINVAL;
+  if (n_items == 0) return PYST_OK;
+  const int bs = run->block_size ? run->block_size : 128;
+  if (bs < 32 || bs > 128 || bs % 32) return PYST_EINVAL;
+  const RunArgs ra = make_args(run);
+  OutBase ob = make_outbase(out, 1);
+  ob.stride = 0;  // per item
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned long long* queue = (unsigned long long*)d_workspace;
+  if (out->score)
+    return launch_batch_1(d_blobs, d_items, n_items, lim, ra, ob, queue, bs,
+                          st);
+  return launch_batch_0(d_blobs, d_items, n_items, lim, ra, ob, queue, bs, st);
+}
+
+int pyst_score_backward_workspace_size(int64_t n_traj, int32_t n_reactions,
+                                       size_t* bytes) {
+  if (!bytes || n_traj < 0 || n_reactions < 1) return PYST_EINVAL;
+  int64_t nblk = score_backward_blocks(n_traj);
+  if (nblk < 1) nblk = 1;
+  *bytes = (size_t)nblk * (size_t)n_reactions * sizeof(double);
+  return PYST_OK;
+}
+
+int pyst_score_backward(const int32_t* samples, const double* score,
+                        int64_t n_traj, int32_t kappa, int32_t ita,
+                        int32_t n_reactions, const double* mean,
+                        const double* var, const double* gmean,
+                        const double* gvar, double* d_grad, void* d_workspace,
+                        size_t workspace_bytes, void* stream) {
+  if (!samples || !score || !mean || !gmean || !d_grad || n_traj < 1 ||
+      kappa < 1 || ita < 1 || n_reactions < 1)
+    return PYST_EINVAL;
+  if (gvar && !var) return PYST_EINVAL;
+  size_t need = 0;
+  pyst_score_backward_workspace_size(n_traj, n_reactions, &need);
+  if (!d_workspace || ((uintptr_t)d_workspace & 7)) return PYST_EINVAL;
+  if (workspace_bytes < need) return PYST_EWORKSPACE;
+  return launch_score_backward(samples, score, n_traj, kappa, ita,
+                               n_reactions, mean, var, gmean, gvar,
+                               (double*)d_workspace, d_grad,
+                               (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,785 @@
+// Per-trajectory simulation engines.
+//
+// Two mappings of one trajectory onto the GPU:
+//   * run_thread<MAXR,...>: one trajectory per thread, for R <= MAXR <= 32.
+//     The propensities a[MAXR] live in registers (loops unrolled over the
+//     compile-time bound and guarded by j < R); species counts live in a
+//     per-thread column of shared memory (element i*bs + lane-of-block).
+//   * run_warp<...>: one trajectory per warp, for any R.  Lanes own
+//     contiguous reaction slices; the total propensity is a Kogge-Stone
+//     prefix sum over the lanes' FP64 partial sums (shuffles) and the firing
+//     reaction is found with a ballot over the lane prefixes.
+//
+// Both restate the reference algorithms:
+//   direct method   mod/simulator/cuGillespie/gillespie.py:70-146,
+//                   mod/simulator/cuTauLeaping/P3.py:71-151
+//   tau-leaping     mod/simulator/cuTauLeaping/P1_P2.py:96-297 with helpers
+//                   299-584; the host rounds of cuTauLeaping.py:49-76 become
+//                   one loop per trajectory (mode DECIDE = P1_P2, mode SSA =
+//                   up to ssa_fallback_steps iterations of P3).
+// Precision: propensities FP32; total propensity, clock, cumulative
+// selection sums and score integrals FP64; tau selection and leap sampling
+// FP32.  Every floating-point operation is explicitly rounded.
+#pragma once
+#include <stdint.h>
+
+#include "pyst_math.cuh"
+#include "pyst_model.cuh"
+
+namespace pyst {
+
+struct RunArgs {
+  uint64_t seed;
+  int64_t step_budget;
+  int32_t ssa_fallback_steps;
+  int32_t max_leap_retries;
+};
+
+// Output pointers of one trajectory (already offset to it).
+struct TrajOut {
+  int32_t* samples;  // element (k*ita + f)*stride
+  int64_t stride;
+  uint8_t* status;
+  int64_t* events;
+  uint64_t* seqhash;
+  double* t_final;
+  double* score;  // [R]
+};
+
+#define PYST_I32MAX 2147483647ll
+#define PYST_LEAP_TAG 0xFFFFFFFFull
+
+__device__ __forceinline__ float gfun(uint32_t gw, int x) {
+  const int H = (int)(gw & 0xFFu);
+  const int Ht = (int)((gw >> 8) & 0xFFu);
+  const float xf = (float)x;
+  if (H == 1) return 1.0f;
+  if (H == 2) {
+    if (Ht == 2) return __fadd_rn(2.0f, __fdiv_rn(1.0f, __fsub_rn(xf, 1.0f)));
+    return 2.0f;
+  }
+  if (H == 3) {
+    if (Ht == 3) {
+      const float t1 = __fdiv_rn(1.0f, __fsub_rn(xf, 1.0f));
+      const float t2 = __fdiv_rn(2.0f, __fsub_rn(xf, 2.0f));
+      return __fadd_rn(__fadd_rn(3.0f, t1), t2);
+    }
+    if (Ht == 2)
+      return __fmul_rn(1.5f,
+                       __fadd_rn(2.0f, __fdiv_rn(1.0f, __fsub_rn(xf, 1.0f))));
+    return 3.0f;
+  }
+  if (H >= 4) {
+    // Cao-Gillespie-Petzold's g generalised past third order (the
+    // reference's CalculateG returns 0 there, P1_P2.py:480-485, which makes
+    // tau infinite): g = (H/n) (n + sum_{k=1}^{n-1} k/(x-k)), n = H_type;
+    // for H <= 3 this is exactly the table above.
+    const int n = Ht < 1 ? 1 : Ht;
+    float sm = (float)n;
+    for (int k = 1; k < n; ++k)
+      sm = __fadd_rn(sm, __fdiv_rn((float)k, __fsub_rn(xf, (float)k)));
+    return __fmul_rn(__fdiv_rn((float)H, (float)n), sm);
+  }
+  return 0.0f;
+}
+
+// Candidate tau of one reactant species (P1_P2.py:421-426), FP32.
+__device__ __forceinline__ float tau_candidate(float eta, uint32_t gw, int x,
+                                               float mu, float s2) {
+  const float g = gfun(gw, x);
+  const float num = fmaxf(__fdiv_rn(__fmul_rn(eta, (float)x), g), 1.0f);
+  const float lhs = __fdiv_rn(num, fabsf(mu));
+  const float rhs = __fdiv_rn(__fmul_rn(num, num), s2);
+  return fminf(lhs, rhs);
+}
+
+__device__ __forceinline__ PoissonKey leap_key(const Stream& s, uint32_t q,
+                                               int j, int retry) {
+  PoissonKey pk;
+  pk.k0 = s.k0;
+  pk.k1 = s.k1;
+  pk.c0 = q;
+  pk.c1 = 0x80000000u | ((uint32_t)j << 12) | ((uint32_t)retry << 6);
+  pk.c2 = s.c2;
+  pk.c3 = s.c3;
+  return pk;
+}
+
+// Propensity of reaction j in FP32 (rate, then factors in entry order).
+template <class XGet>
+__device__ __forceinline__ float propensity(const ModelView& m, int j,
+                                            XGet xget) {
+  float a = m.rate(j);
+  const int e1 = m.facptr(j + 1);
+  for (int e = m.facptr(j); e < e1; ++e) {
+    const uint32_t fe = m.fac(e);
+    const int x = xget(ent_lo(fe));
+    const int n = fac_order(fe);
+    const int fall = fac_falling(fe);
+    for (int q = 0; q < n; ++q) a = __fmul_rn(a, (float)(x - q * fall));
+  }
+  return a;
+}
+
+__device__ __forceinline__ void store_sample(const TrajOut& o, int ita, int k,
+                                             int f, int32_t v) {
+  o.samples[((int64_t)k * ita + f) * o.stride] = v;
+}
+
+// ===================================================================
+// one trajectory per thread
+// ===================================================================
+template <int MAXR, bool TAU, bool SCORE>
+__device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
+                           int bs, const RunArgs& ra, uint64_t traj_id,
+                           const TrajOut& o) {
+  const int S = m.S, R = m.R, ita = m.ita, kappa = m.kappa;
+#define XV(i) xcol[(int64_t)(i) * bs]
+#define SL(i) slot[(int64_t)(i) * bs]
+  for (int i = 0; i < S; ++i) XV(i) = m.x0(i);
+  Stream rs = make_stream(ra.seed, traj_id);
+  double t = 0.0;
+  int f = 0;
+  int64_t events = 0, steps = 0;
+  uint64_t h = PYST_FNV_OFFSET;
+  int status = PYST_TRAJ_DONE;
+  bool fill_state = false;
+  const int64_t budget = ra.step_budget;
+  const double t_end = m.time(ita - 1);
+  double integ[SCORE ? MAXR : 1];
+  int cnt[SCORE ? MAXR : 1];
+  if (SCORE) {
+#pragma unroll
+    for (int j = 0; j < MAXR; ++j) {
+      integ[j] = 0.0;
+      cnt[j] = 0;
+    }
+  }
+  bool ssa_mode = !TAU;
+  int ssa_left = 0;
+  uint32_t leap_q = 0;
+  auto xget = [&](int i) { return XV(i); };
+
+  while (true) {
+    float a[MAXR];
+    double a0 = 0.0;
+#pragma unroll
+    for (int j = 0; j < MAXR; ++j) {
+      if (j >= R) break;
+      a[j] = propensity(m, j, xget);
+      a0 = __dadd_rn(a0, (double)a[j]);
+    }
+    if (a0 == 0.0) {
+      status = PYST_TRAJ_ABSORBED;
+      fill_state = true;
+      break;
+    }
+    if (steps >= budget) {
+      status = PYST_TRAJ_STEP_BUDGET;
+      break;
+    }
+    if (TAU && !ssa_mode) {
+      // ---------------- DECIDE: critical set, tau_1, SSA switch -------
+      uint32_t crit = 0u;
+#pragma unroll
+      for (int j = 0; j < MAXR; ++j) {
+        if (j >= R) break;
+        const int e1 = m.critptr(j + 1);
+        for (int e = m.critptr(j); e < e1; ++e) {
+          const uint32_t ce = m.crit(e);
+          if ((int64_t)(ce >> 16) * m.n_c > (int64_t)XV(ent_lo(ce)))
+            crit |= 1u << j;
+        }
+      }
+      for (int i = 0; i < S; ++i) SL(i) = 0;
+#pragma unroll
+      for (int j = 0; j < MAXR; ++j) {
+        if (j >= R) break;
+        if (!((crit >> j) & 1u)) {
+          const int e1 = m.netptr(j + 1);
+          for (int e = m.netptr(j); e < e1; ++e) {
+            const uint32_t ne = m.net(e);
+            const int sp = ent_lo(ne);
+            const int v = ent_hi_s16(ne);
+            float2 ms = *reinterpret_cast<float2*>(&SL(sp));
+            ms.x = __fadd_rn(ms.x, __fmul_rn((float)v, a[j]));
+            ms.y = __fadd_rn(ms.y, __fmul_rn((float)(v * v), a[j]));
+            *reinterpret_cast<float2*>(&SL(sp)) = ms;
+          }
+        }
+      }
+      float tau1 = __int_as_float(0x7f800000);
+      for (int i = 0; i < S; ++i) {
+        const uint32_t gw = m.g(i);
+        if (!((gw >> 16) & 1u)) continue;
+        const float2 ms = *reinterpret_cast<float2*>(&SL(i));
+        const float c = tau_candidate(m.eta, gw, XV(i), ms.x, ms.y);
+        if (c < tau1) tau1 = c;
+      }
+      if ((double)tau1 < __ddiv_rn(10.0, a0)) {
+        ssa_mode = true;
+        ssa_left = ra.ssa_fallback_steps;
+        // fall through to the SSA step below with the same propensities
+      } else {
+        // ---------------- leap ---------------------------------------
+        steps++;
+        double a0c = 0.0;
+#pragma unroll
+        for (int j = 0; j < MAXR; ++j) {
+          if (j >= R) break;
+          if ((crit >> j) & 1u) a0c = __dadd_rn(a0c, (double)a[j]);
+        }
+        double tau2 = __longlong_as_double(0x7ff0000000000000ll);
+        uint4 wc = make_uint4(0, 0, 0, 0);
+        if (a0c > 0.0) {
+          wc = next_block(rs);
+          tau2 = __ddiv_rn(-pyst_log(u53(wc.x, wc.y)), a0c);
+        }
+        const double tau1d = (double)tau1;
+        double tau = (tau2 < tau1d) ? tau2 : tau1d;
+        int kcrit = -1;
+        if (tau1d > tau2) {
+          const double r = __dmul_rn(u53(wc.z, wc.w), a0c);
+          double cum = 0.0;
+          int lastnz = -1;
+#pragma unroll
+          for (int j = 0; j < MAXR; ++j) {
+            if (j >= R) break;
+            if ((crit >> j) & 1u) {
+              cum = __dadd_rn(cum, (double)a[j]);
+              if (a[j] > 0.0f) lastnz = j;
+              if (cum >= r) {
+                kcrit = j;
+                break;
+              }
+            }
+          }
+          if (kcrit < 0) kcrit = lastnz;
+        }
+        int K[MAXR];
+        int retry = 0;
+        bool ok = false;
+        while (true) {
+          bool bad = false;
+#pragma unroll
+          for (int j = 0; j < MAXR; ++j) {
+            if (j >= R) break;
+            if ((crit >> j) & 1u) {
+              K[j] = (j == kcrit) ? 1 : 0;
+            } else {
+              const float lam = __fmul_rn(a[j], (float)tau);
+              const int k = poisson(lam, leap_key(rs, leap_q, j, retry));
+              if (k < 0) bad = true;
+              K[j] = k < 0 ? 0 : k;
+            }
+          }
+          if (bad) {
+            status = PYST_TRAJ_SAMPLER;
+            break;
+          }
+          for (int i = 0; i < S; ++i) SL(i) = 0;
+#pragma unroll
+          for (int j = 0; j < MAXR; ++j) {
+            if (j >= R) break;
+            if (K[j] != 0) {
+              const int e1 = m.netptr(j + 1);
+              for (int e = m.netptr(j); e < e1; ++e) {
+                const uint32_t ne = m.net(e);
+                SL(ent_lo(ne)) += (int64_t)K[j] * ent_hi_s16(ne);
+              }
+            }
+          }
+          bool neg = false, over = false;
+          for (int i = 0; i < S; ++i) {
+            const int64_t nx = (int64_t)XV(i) + SL(i);
+            neg |= nx < 0;
+            over |= nx > PYST_I32MAX;
+          }
+          if (over) {
+            status = PYST_TRAJ_OVERFLOW;
+            break;
+          }
+          if (!neg) {
+            ok = true;
+            break;
+          }
+          tau = __dmul_rn(tau, 0.5);
+          retry++;
+          if (retry > ra.max_leap_retries) {
+            status = PYST_TRAJ_LEAP_RETRY;
+            break;
+          }
+        }
+        if (!ok) break;
+        leap_q++;
+        const double tn = __dadd_rn(t, tau);
+        int64_t fired = 0;
+        h = seq_mix(h, PYST_LEAP_TAG);
+#pragma unroll
+        for (int j = 0; j < MAXR; ++j) {
+          if (j >= R) break;
+          fired += K[j];
+          if (K[j] != 0) h = seq_mix(h, ((uint64_t)j << 32) | (uint32_t)K[j]);
+          if (SCORE) {
+            cnt[j] += K[j];
+            integ[j] = __dadd_rn(integ[j], __dmul_rn((double)a[j], tau));
+          }
+        }
+        bool done = false;
+        while (tn >= m.time(f)) {
+          const double frac = __ddiv_rn(__dsub_rn(m.time(f), t), tau);
+          for (int k = 0; k < kappa; ++k) {
+            const int i = m.out(k);
+            const double inc = rint(__dmul_rn((double)SL(i), frac));
+            store_sample(o, ita, k, f, XV(i) + (int)inc);
+          }
+          f++;
+          if (f == ita) {
+            done = true;
+            break;
+          }
+        }
+        for (int i = 0; i < S; ++i) XV(i) = (int)((int64_t)XV(i) + SL(i));
+        events += fired;
+        t = tn;
+        if (done) break;
+        continue;
+      }
+    }
+    // ------------------------ one direct-method step -------------------
+    steps++;
+    const uint4 w = next_block(rs);
+    const double tau = __ddiv_rn(-pyst_log(u53(w.x, w.y)), a0);
+    const double r = __dmul_rn(u53(w.z, w.w), a0);
+    int sel = -1;
+    {
+      double cum = 0.0;
+      int lastnz = -1;
+#pragma unroll
+      for (int j = 0; j < MAXR; ++j) {
+        if (j >= R) break;
+        cum = __dadd_rn(cum, (double)a[j]);
+        if (a[j] > 0.0f) lastnz = j;
+        if (cum >= r) {
+          sel = j;
+          break;
+        }
+      }
+      // unreachable in exact arithmetic (the last sum equals a0 >= r);
+      // kept so a selection always names a reaction with a_j > 0
+      if (sel < 0) sel = lastnz;
+    }
+    const double tn = __dadd_rn(t, tau);
+    if (SCORE) {
+      const double dt = (tn >= t_end) ? __dsub_rn(t_end, t) : tau;
+#pragma unroll
+      for (int j = 0; j < MAXR; ++j) {
+        if (j >= R) break;
+        integ[j] = __dadd_rn(integ[j], __dmul_rn((double)a[j], dt));
+      }
+    }
+    bool done = false;
+    while (tn >= m.time(f)) {
+      for (int k = 0; k < kappa; ++k) store_sample(o, ita, k, f, XV(m.out(k)));
+      f++;
+      if (f == ita) {
+        done = true;
+        break;
+      }
+    }
+    t = tn;
+    if (done) break;
+    {
+      const int e1 = m.netptr(sel + 1);
+      bool over = false;
+      for (int e = m.netptr(sel); e < e1; ++e) {
+        const uint32_t ne = m.net(e);
+        const int sp = ent_lo(ne);
+        const int64_t nx = (int64_t)XV(sp) + ent_hi_s16(ne);
+        if (nx < 0 || nx > PYST_I32MAX) over = true;
+        else XV(sp) = (int)nx;
+      }
+      if (over) {
+        status = PYST_TRAJ_OVERFLOW;
+        break;
+      }
+    }
+    events++;
+    h = seq_mix(h, (uint64_t)sel);
+    if (SCORE) {
+#pragma unroll
+      for (int j = 0; j < MAXR; ++j) cnt[j] += (j == sel) ? 1 : 0;
+    }
+    if (TAU) {
+      if (--ssa_left <= 0) ssa_mode = false;
+    }
+  }
+  // remaining samples: state after absorption, -1 after an error
+  for (; f < ita; ++f)
+    for (int k = 0; k < kappa; ++k)
+      store_sample(o, ita, k, f, fill_state ? XV(m.out(k)) : -1);
+  if (o.status) *o.status = (uint8_t)status;
+  if (o.events) *o.events = events;
+  if (o.seqhash) *o.seqhash = h;
+  if (o.t_final) *o.t_final = t;
+  if (SCORE && o.score) {
+#pragma unroll
+    for (int j = 0; j < MAXR; ++j) {
+      if (j >= R) break;
+      o.score[j] = __dsub_rn((double)cnt[j], integ[j]);
+    }
+  }
+#undef XV
+#undef SL
+}
+
+// ===================================================================
+// one trajectory per warp
+// ===================================================================
+// Per-warp shared memory: x[S] int32, a[R] float, slot[S] 8 bytes,
+// K[R] int32, crit[R] uint8 (rounded up to 4).  Lane l owns reactions
+// [l*c, min(R,(l+1)*c)) with c = ceil(R/32); it owns species l, l+32, ...
+struct WarpSmem {
+  int32_t* x;
+  float* a;
+  int64_t* slot;
+  int32_t* K;
+  uint8_t* crit;
+};
+
+__device__ __forceinline__ size_t warp_smem_bytes(int S, int R) {
+  size_t b = (size_t)S * 8 + (size_t)S * 4 + (size_t)R * 4 + (size_t)R * 4 +
+             (((size_t)R + 3) & ~(size_t)3);
+  return (b + 15) & ~(size_t)15;
+}
+
+__device__ __forceinline__ WarpSmem warp_smem(void* base, int S, int R) {
+  WarpSmem w;
+  char* p = (char*)base;
+  w.slot = (int64_t*)p;
+  p += (size_t)S * 8;
+  w.x = (int32_t*)p;
+  p += (size_t)S * 4;
+  w.a = (float*)p;
+  p += (size_t)R * 4;
+  w.K = (int32_t*)p;
+  p += (size_t)R * 4;
+  w.crit = (uint8_t*)p;
+  return w;
+}
+
+// Kogge-Stone inclusive scan of lane partial sums (FP64).  The oracle's
+// warp mode repeats exactly these additions.
+__device__ __forceinline__ double warp_incl_scan(double v, int lane) {
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const double n = __shfl_up_sync(0xffffffffu, v, d);
+    if (lane >= d) v = __dadd_rn(n, v);
+  }
+  return v;
+}
+
+// Select within lane prefixes: first lane L with p_L > 0 and incl_L >= r
+// (fallback: last lane with p > 0); inside L, with r' = r - (incl_L - p_L),
+// the first owned j whose running sum reaches r' (fallback: last owned j
+// with a_j > 0).  Returns j on every lane.
+__device__ __forceinline__ int warp_select(const float* a, double part,
+                                          double incl, double r, int j0,
+                                          int j1, int lane,
+                                          const uint8_t* mask) {
+  const unsigned hit = __ballot_sync(0xffffffffu, part > 0.0 && incl >= r);
+  const unsigned nz = __ballot_sync(0xffffffffu, part > 0.0);
+  const int L = hit ? (__ffs(hit) - 1) : (31 - __clz(nz));
+  int sel = -1;
+  if (lane == L) {
+    const double rr = __dsub_rn(r, __dsub_rn(incl, part));
+    double cum = 0.0;
+    int lastnz = -1;
+    for (int j = j0; j < j1; ++j) {
+      if (mask && !mask[j]) continue;
+      const float aj = a[j];
+      cum = __dadd_rn(cum, (double)aj);
+      if (aj > 0.0f) lastnz = j;
+      if (cum >= rr) {
+        sel = j;
+        break;
+      }
+    }
+    if (sel < 0) sel = lastnz;
+  }
+  return __shfl_sync(0xffffffffu, sel, L);
+}
+
+template <bool TAU, bool SCORE>
+__device__ void run_warp(const ModelView& m, const WarpSmem& ws,
+                         const RunArgs& ra, uint64_t traj_id, const TrajOut& o,
+                         double* score_acc /* per-warp [R] or null */) {
+  const int S = m.S, R = m.R, ita = m.ita, kappa = m.kappa;
+  const int lane = threadIdx.x & 31;
+  const int c = (R + 31) >> 5;
+  const int j0 = min(R, lane * c), j1 = min(R, j0 + c);
+  for (int i = lane; i < S; i += 32) ws.x[i] = m.x0(i);
+  if (SCORE)
+    for (int j = lane; j < R; j += 32) score_acc[j] = 0.0;
+  __syncwarp();
+  Stream rs = make_stream(ra.seed, traj_id);
+  double t = 0.0;
+  int f = 0;
+  int64_t events = 0, steps = 0;
+  uint64_t h = PYST_FNV_OFFSET;
+  int status = PYST_TRAJ_DONE;
+  bool fill_state = false;
+  const double t_end = m.time(ita - 1);
+  bool ssa_mode = !TAU;
+  int ssa_left = 0;
+  uint32_t leap_q = 0;
+  auto xget = [&](int i) { return ws.x[i]; };
+
+  while (true) {
+    double part = 0.0;
+    for (int j = j0; j < j1; ++j) {
+      const float aj = propensity(m, j, xget);
+      ws.a[j] = aj;
+      part = __dadd_rn(part, (double)aj);
+    }
+    const double incl = warp_incl_scan(part, lane);
+    const double a0 = __shfl_sync(0xffffffffu, incl, 31);
+    __syncwarp();
+    if (a0 == 0.0) {
+      status = PYST_TRAJ_ABSORBED;
+      fill_state = true;
+      break;
+    }
+    if (steps >= ra.step_budget) {
+      status = PYST_TRAJ_STEP_BUDGET;
+      break;
+    }
+    if (TAU && !ssa_mode) {
+      // critical flags for owned reactions
+      for (int j = j0; j < j1; ++j) {
+        uint8_t cf = 0;
+        const int e1 = m.critptr(j + 1);
+        for (int e = m.critptr(j); e < e1; ++e) {
+          const uint32_t ce = m.crit(e);
+          if ((int64_t)(ce >> 16) * m.n_c > (int64_t)ws.x[ent_lo(ce)]) cf = 1;
+        }
+        ws.crit[j] = cf;
+      }
+      __syncwarp();
+      // mu, sigma^2 and the tau candidate per owned species
+      float tmin = __int_as_float(0x7f800000);
+      for (int i = lane; i < S; i += 32) {
+        const uint32_t gw = m.g(i);
+        if (!((gw >> 16) & 1u)) continue;
+        float mu = 0.0f, s2 = 0.0f;
+        const int e1 = m.spvptr(i + 1);
+        for (int e = m.spvptr(i); e < e1; ++e) {
+          const uint32_t se = m.spv(e);
+          const int j = ent_lo(se);
+          if (ws.crit[j]) continue;
+          const int v = ent_hi_s16(se);
+          mu = __fadd_rn(mu, __fmul_rn((float)v, ws.a[j]));
+          s2 = __fadd_rn(s2, __fmul_rn((float)(v * v), ws.a[j]));
+        }
+        const float cnd = tau_candidate(m.eta, gw, ws.x[i], mu, s2);
+        if (cnd < tmin) tmin = cnd;
+      }
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1)
+        tmin = fminf(tmin, __shfl_xor_sync(0xffffffffu, tmin, d));
+      const float tau1 = tmin;
+      if ((double)tau1 < __ddiv_rn(10.0, a0)) {
+        ssa_mode = true;
+        ssa_left = ra.ssa_fallback_steps;
+      } else {
+        steps++;
+        double pc = 0.0;
+        for (int j = j0; j < j1; ++j)
+          if (ws.crit[j]) pc = __dadd_rn(pc, (double)ws.a[j]);
+        const double inc_c = warp_incl_scan(pc, lane);
+        const double a0c = __shfl_sync(0xffffffffu, inc_c, 31);
+        double tau2 = __longlong_as_double(0x7ff0000000000000ll);
+        uint4 wc = make_uint4(0, 0, 0, 0);
+        if (a0c > 0.0) {
+          wc = next_block(rs);
+          tau2 = __ddiv_rn(-pyst_log(u53(wc.x, wc.y)), a0c);
+        }
+        const double tau1d = (double)tau1;
+        double tau = (tau2 < tau1d) ? tau2 : tau1d;
+        int kcrit = -1;
+        if (tau1d > tau2) {
+          const double r = __dmul_rn(u53(wc.z, wc.w), a0c);
+          kcrit = warp_select(ws.a, pc, inc_c, r, j0, j1, lane, ws.crit);
+        }
+        int retry = 0;
+        bool ok = false;
+        while (true) {
+          bool bad = false;
+          for (int j = j0; j < j1; ++j) {
+            int kj = 0;
+            if (ws.crit[j]) {
+              kj = (j == kcrit) ? 1 : 0;
+            } else {
+              const float lam = __fmul_rn(ws.a[j], (float)tau);
+              const int k = poisson(lam, leap_key(rs, leap_q, j, retry));
+              if (k < 0) bad = true;
+              kj = k < 0 ? 0 : k;
+            }
+            ws.K[j] = kj;
+          }
+          for (int i = lane; i < S; i += 32) ws.slot[i] = 0;
+          __syncwarp();
+          if (__any_sync(0xffffffffu, bad)) {
+            status = PYST_TRAJ_SAMPLER;
+            break;
+          }
+          // species-major accumulation of V K (lane owns species)
+          bool neg = false, over = false;
+          for (int i = lane; i < S; i += 32) {
+            int64_t d = 0;
+            const int e1 = m.spvptr(i + 1);
+            const uint32_t gw = m.g(i);
+            (void)gw;
+            for (int e = m.spvptr(i); e < e1; ++e) {
+              const uint32_t se = m.spv(e);
+              d += (int64_t)ws.K[ent_lo(se)] * ent_hi_s16(se);
+            }
+            ws.slot[i] = d;
+            const int64_t nx = (int64_t)ws.x[i] + d;
+            neg |= nx < 0;
+            over |= nx > PYST_I32MAX;
+          }
+          __syncwarp();
+          if (__any_sync(0xffffffffu, over)) {
+            status = PYST_TRAJ_OVERFLOW;
+            break;
+          }
+          if (!__any_sync(0xffffffffu, neg)) {
+            ok = true;
+            break;
+          }
+          tau = __dmul_rn(tau, 0.5);
+          retry++;
+          if (retry > ra.max_leap_retries) {
+            status = PYST_TRAJ_LEAP_RETRY;
+            break;
+          }
+        }
+        if (!ok) break;
+        leap_q++;
+        const double tn = __dadd_rn(t, tau);
+        // firing count and hash (lane 0 walks K in order)
+        int64_t fired = 0;
+        for (int j = j0; j < j1; ++j) {
+          fired += ws.K[j];
+          if (SCORE) {
+            score_acc[j] = __dadd_rn(score_acc[j], (double)ws.K[j]);
+          }
+        }
+        if (SCORE) {
+          for (int j = j0; j < j1; ++j) {
+            // integral term kept in a separate pass of the same slot
+            score_acc[R + j] =
+                __dadd_rn(score_acc[R + j], __dmul_rn((double)ws.a[j], tau));
+          }
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1)
+          fired += __shfl_xor_sync(0xffffffffu, fired, d);
+        if (lane == 0) {
+          h = seq_mix(h, PYST_LEAP_TAG);
+          for (int j = 0; j < R; ++j)
+            if (ws.K[j] != 0)
+              h = seq_mix(h, ((uint64_t)j << 32) | (uint32_t)ws.K[j]);
+        }
+        bool done = false;
+        while (tn >= m.time(f)) {
+          const double frac = __ddiv_rn(__dsub_rn(m.time(f), t), tau);
+          for (int k = lane; k < kappa; k += 32) {
+            const int i = m.out(k);
+            const double inc = rint(__dmul_rn((double)ws.slot[i], frac));
+            store_sample(o, ita, k, f, ws.x[i] + (int)inc);
+          }
+          f++;
+          if (f == ita) {
+            done = true;
+            break;
+          }
+        }
+        __syncwarp();
+        for (int i = lane; i < S; i += 32)
+          ws.x[i] = (int)((int64_t)ws.x[i] + ws.slot[i]);
+        __syncwarp();
+        events += fired;
+        t = tn;
+        if (done) break;
+        continue;
+      }
+    }
+    // ------------------------ one direct-method step -------------------
+    steps++;
+    const uint4 w = next_block(rs);
+    const double tau = __ddiv_rn(-pyst_log(u53(w.x, w.y)), a0);
+    const double r = __dmul_rn(u53(w.z, w.w), a0);
+    const int sel = warp_select(ws.a, part, incl, r, j0, j1, lane, nullptr);
+    const double tn = __dadd_rn(t, tau);
+    if (SCORE) {
+      const double dt = (tn >= t_end) ? __dsub_rn(t_end, t) : tau;
+      for (int j = j0; j < j1; ++j)
+        score_acc[R + j] =
+            __dadd_rn(score_acc[R + j], __dmul_rn((double)ws.a[j], dt));
+    }
+    bool done = false;
+    while (tn >= m.time(f)) {
+      for (int k = lane; k < kappa; k += 32)
+        store_sample(o, ita, k, f, ws.x[m.out(k)]);
+      f++;
+      if (f == ita) {
+        done = true;
+        break;
+      }
+    }
+    t = tn;
+    if (done) break;
+    bool over = false;
+    if (lane == 0) {
+      const int e1 = m.netptr(sel + 1);
+      for (int e = m.netptr(sel); e < e1; ++e) {
+        const uint32_t ne = m.net(e);
+        const int sp = ent_lo(ne);
+        const int64_t nx = (int64_t)ws.x[sp] + ent_hi_s16(ne);
+        if (nx < 0 || nx > PYST_I32MAX) over = true;
+        else ws.x[sp] = (int)nx;
+      }
+      if (SCORE) score_acc[sel] = __dadd_rn(score_acc[sel], 1.0);
+    }
+    __syncwarp();
+    if (__any_sync(0xffffffffu, over)) {
+      status = PYST_TRAJ_OVERFLOW;
+      break;
+    }
+    events++;
+    h = seq_mix(h, (uint64_t)sel);
+    if (TAU) {
+      if (--ssa_left <= 0) ssa_mode = false;
+    }
+  }
+  __syncwarp();
+  for (; f < ita; ++f)
+    for (int k = lane; k < kappa; k += 32)
+      store_sample(o, ita, k, f, fill_state ? ws.x[m.out(k)] : -1);
+  if (lane == 0) {
+    if (o.status) *o.status = (uint8_t)status;
+    if (o.events) *o.events = events;
+    if (o.seqhash) *o.seqhash = h;
+    if (o.t_final) *o.t_final = t;
+  }
+  if (SCORE && o.score) {
+    __syncwarp();
+    for (int j = lane; j < R; j += 32)
+      o.score[j] = __dsub_rn(score_acc[j], score_acc[R + j]);
+  }
+  __syncwarp();
+}
+
+}  // namespace pyst

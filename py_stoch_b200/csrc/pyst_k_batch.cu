@@ -1,0 +1,112 @@
+// Batched persistent kernel: many models of uneven size in one launch.
+// Blocks take work items (one model, its trajectories and output offsets)
+// from a device queue (an atomic counter in caller workspace), stage the
+// item's model blob into shared memory with one bulk-async copy, and run its
+// trajectories thread-per-trajectory or warp-per-trajectory as the item
+// says.  Replaces the reference's one-JIT-and-launch-sequence-per-model
+// sweep (examples/*_sim.py loops over CuTauLeaping().run, e.g.
+// examples/schlogl_sim.py:66-80).  Built once per PYST_SCORE flavour.
+#include "pyst_launch.cuh"
+
+namespace pyst {
+namespace {
+
+template <bool SCORE>
+__global__ void __launch_bounds__(128)
+    k_batch(const uint32_t* __restrict__ gblobs,
+            const pyst_batch_item* __restrict__ items, int64_t n_items,
+            RunArgs ra, OutBase ob, unsigned long long* queue,
+            int max_blob_words, int warp_bytes) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ long long s_item;
+  uint32_t* sblob = (uint32_t*)smem;
+  uint64_t* bar = (uint64_t*)(smem + (size_t)max_blob_words * 4);
+  unsigned char* dyn = smem + (size_t)max_blob_words * 4 + 16;
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const int bs = blockDim.x, nw = bs >> 5, wid = threadIdx.x >> 5;
+  uint32_t parity = 0;
+  while (true) {
+    if (threadIdx.x == 0) s_item = (long long)atomicAdd(queue, 1ull);
+    __syncthreads();
+    const long long it = s_item;
+    if (it >= n_items) break;
+    const pyst_batch_item item = items[it];
+    const uint32_t* blob = gblobs + item.blob_offset;
+    const int words = (int)__ldg(blob + PYST_H_WORDS);
+    const bool ok = stage_blob(sblob, blob, words, bar, parity);
+    if (!ok) {
+      mbar_wait(bar, parity);
+      for (int64_t u = threadIdx.x; u < item.n_traj; u += bs)
+        mark_staging_failure(ob, item.traj_offset + u);
+      break;
+    }
+    parity ^= 1u;
+    ModelView m;
+    m.load(sblob);
+    const bool tau = item.method == PYST_METHOD_TAU_LEAP;
+    if (item.mapping == PYST_MAP_THREAD) {
+      int32_t* xcol = (int32_t*)dyn + threadIdx.x;
+      int64_t* slot =
+          (int64_t*)((int32_t*)dyn + (size_t)m.S * bs) + threadIdx.x;
+      for (int64_t u = threadIdx.x; u < item.n_traj; u += bs) {
+        const TrajOut o = ob.at(item.sample_offset, u, item.traj_offset,
+                                item.score_offset, item.n_traj, m.R);
+        const uint64_t id = (uint64_t)item.traj_id_base + (uint64_t)u;
+        if (m.R <= 8) {
+          if (tau) run_thread<8, true, SCORE>(m, xcol, slot, bs, ra, id, o);
+          else run_thread<8, false, SCORE>(m, xcol, slot, bs, ra, id, o);
+        } else {
+          if (tau) run_thread<32, true, SCORE>(m, xcol, slot, bs, ra, id, o);
+          else run_thread<32, false, SCORE>(m, xcol, slot, bs, ra, id, o);
+        }
+      }
+    } else {
+      unsigned char* mine = dyn + (size_t)wid * warp_bytes;
+      const WarpSmem ws = warp_smem(mine, m.S, m.R);
+      double* sacc = (double*)(mine + warp_smem_bytes(m.S, m.R));
+      for (int64_t u = wid; u < item.n_traj; u += nw) {
+        const TrajOut o = ob.at(item.sample_offset, u, item.traj_offset,
+                                item.score_offset, item.n_traj, m.R);
+        const uint64_t id = (uint64_t)item.traj_id_base + (uint64_t)u;
+        if (tau) run_warp<true, SCORE>(m, ws, ra, id, o, sacc);
+        else run_warp<false, SCORE>(m, ws, ra, id, o, sacc);
+      }
+    }
+    __syncthreads();  // everyone done with sblob and dyn before restaging
+  }
+}
+
+}  // namespace
+
+int PYST_CAT(launch_batch_, PYST_SCORE, )(
+    const uint32_t* d_blobs, const pyst_batch_item* d_items, int64_t n_items,
+    const pyst_batch_limits* lim, const RunArgs& ra, const OutBase& ob,
+    unsigned long long* queue, int bs, cudaStream_t st) {
+  const size_t wb =
+      host_warp_bytes(lim->max_species, lim->max_reactions, PYST_SCORE);
+  const size_t thread_bytes = (size_t)bs * lim->max_species * 12;
+  const size_t wbytes = wb * (size_t)(bs / 32);
+  const size_t dyn = thread_bytes > wbytes ? thread_bytes : wbytes;
+  const size_t smem = (size_t)lim->max_blob_words * 4 + 16 + dyn;
+  if (smem > kMaxDynSmem) return PYST_EUNSUPPORTED;
+  auto kf = k_batch<(bool)PYST_SCORE>;
+  const int rc = set_smem(kf, smem);
+  if (rc) return rc;
+  if (cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st) !=
+      cudaSuccess)
+    return PYST_ECUDA;
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf, bs, smem);
+  if (per_sm < 1) per_sm = 1;
+  int64_t grid = (int64_t)num_sms() * per_sm;
+  if (grid > n_items) grid = n_items;
+  kf<<<(unsigned)grid, bs, smem, st>>>(d_blobs, d_items, n_items, ra, ob,
+                                       queue, lim->max_blob_words, (int)wb);
+  return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
+}
+
+}  // namespace pyst

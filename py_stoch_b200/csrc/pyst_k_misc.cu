@@ -1,0 +1,169 @@
+// Likelihood-ratio gradient reduction and the test hooks.
+#include <curand_kernel.h>
+
+#include "pyst_launch.cuh"
+#include "pystoch_b200_testing.h"
+
+namespace pyst {
+namespace {
+
+#define PYST_BWD_CHUNK 256
+
+// h_u for a chunk of trajectories, then per-block partial sums
+// part[block][j] = sum_{u in chunk} h_u score[u][j] in trajectory order.
+__global__ void __launch_bounds__(PYST_BWD_CHUNK)
+    k_score_partial(const int32_t* __restrict__ samples,
+                    const double* __restrict__ score, int64_t U, int kappa,
+                    int ita, int R, const double* __restrict__ mean,
+                    const double* __restrict__ var,
+                    const double* __restrict__ gmean,
+                    const double* __restrict__ gvar, double* part) {
+  __shared__ double hs[PYST_BWD_CHUNK];
+  const int64_t u0 = blockIdx.x * (int64_t)PYST_BWD_CHUNK;
+  const int64_t u = u0 + threadIdx.x;
+  double h = 0.0;
+  if (u < U) {
+    const int KF = kappa * ita;
+    for (int kf = 0; kf < KF; ++kf) {
+      const double d =
+          __dsub_rn((double)samples[(int64_t)kf * U + u], mean[kf]);
+      h = __dadd_rn(h, __dmul_rn(gmean[kf], d));
+      if (gvar)
+        h = __dadd_rn(
+            h, __dmul_rn(gvar[kf], __dsub_rn(__dmul_rn(d, d), var[kf])));
+    }
+  }
+  hs[threadIdx.x] = h;
+  __syncthreads();
+  const int64_t rem = U - u0;
+  const int n = (int)(rem < PYST_BWD_CHUNK ? rem : PYST_BWD_CHUNK);
+  for (int j = threadIdx.x; j < R; j += PYST_BWD_CHUNK) {
+    double acc = 0.0;
+    for (int q = 0; q < n; ++q)
+      acc = __dadd_rn(acc, __dmul_rn(hs[q], score[(u0 + q) * R + j]));
+    part[(int64_t)blockIdx.x * R + j] = acc;
+  }
+}
+
+__global__ void k_score_final(const double* __restrict__ part, int nblk, int R,
+                              int64_t U, double* grad) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < R;
+       j += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int b = 0; b < nblk; ++b)
+      acc = __dadd_rn(acc, part[(int64_t)b * R + j]);
+    grad[j] = __ddiv_rn(acc, (double)U);
+  }
+}
+
+__global__ void k_philox(uint64_t seed, uint64_t id, uint64_t n0,
+                         int64_t count, uint32_t* out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  Stream s = make_stream(seed, id);
+  s.n = n0 + (uint64_t)i;
+  const uint4 r = next_block(s);
+  out[4 * i + 0] = r.x;
+  out[4 * i + 1] = r.y;
+  out[4 * i + 2] = r.z;
+  out[4 * i + 3] = r.w;
+}
+
+__global__ void k_philox_raw(const uint32_t* ctr_key, int64_t count,
+                             uint32_t* out, int use_curand) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const uint32_t* c = ctr_key + 6 * i;
+  uint4 r;
+  if (use_curand)
+    r = curand_Philox4x32_10(make_uint4(c[0], c[1], c[2], c[3]),
+                             make_uint2(c[4], c[5]));
+  else
+    r = philox4x32_10(c[0], c[1], c[2], c[3], c[4], c[5]);
+  out[4 * i + 0] = r.x;
+  out[4 * i + 1] = r.y;
+  out[4 * i + 2] = r.z;
+  out[4 * i + 3] = r.w;
+}
+
+__global__ void k_math(const double* x, int64_t n, int which, double* out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v = 0.0;
+  if (which == 0) v = pyst_log(x[i]);
+  else if (which == 1) v = pyst_exp(x[i]);
+  else if (which == 2) v = pyst_logfact(x[i]);
+  else if (which == 3) v = log(x[i]);
+  else if (which == 4) v = exp(x[i]);
+  out[i] = v;
+}
+
+__global__ void k_poisson(const float* lam, int64_t n, uint64_t seed,
+                          int32_t* out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Stream s = make_stream(seed, (uint64_t)i);
+  out[i] = poisson(lam[i], leap_key(s, 7u, (int)(i & 1023), 3));
+}
+
+}  // namespace
+
+int64_t score_backward_blocks(int64_t U) {
+  return (U + PYST_BWD_CHUNK - 1) / PYST_BWD_CHUNK;
+}
+
+int launch_score_backward(const int32_t* samples, const double* score,
+                          int64_t U, int kappa, int ita, int R,
+                          const double* mean, const double* var,
+                          const double* gmean, const double* gvar,
+                          double* part, double* grad, cudaStream_t st) {
+  const int64_t nblk = score_backward_blocks(U);
+  k_score_partial<<<(unsigned)nblk, PYST_BWD_CHUNK, 0, st>>>(
+      samples, score, U, kappa, ita, R, mean, var, gmean, gvar, part);
+  k_score_final<<<(R + 127) / 128, 128, 0, st>>>(part, (int)nblk, R, U, grad);
+  return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
+}
+
+}  // namespace pyst
+
+using namespace pyst;
+
+extern "C" {
+
+int pyst_test_philox(uint64_t seed, uint64_t id, uint64_t n0, int64_t count,
+                     uint32_t* d_out, void* stream) {
+  if (count <= 0) return PYST_OK;
+  if (!d_out) return PYST_EINVAL;
+  k_philox<<<(unsigned)((count + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+      seed, id, n0, count, d_out);
+  return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
+}
+
+int pyst_test_philox_raw(const uint32_t* d_ctr_key, int64_t count,
+                         uint32_t* d_out, int use_curand, void* stream) {
+  if (count <= 0) return PYST_OK;
+  if (!d_ctr_key || !d_out) return PYST_EINVAL;
+  k_philox_raw<<<(unsigned)((count + 127) / 128), 128, 0,
+                 (cudaStream_t)stream>>>(d_ctr_key, count, d_out, use_curand);
+  return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
+}
+
+int pyst_test_math(const double* d_x, int64_t n, int which, double* d_out,
+                   void* stream) {
+  if (n <= 0) return PYST_OK;
+  if (!d_x || !d_out || which < 0 || which > 4) return PYST_EINVAL;
+  k_math<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+      d_x, n, which, d_out);
+  return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
+}
+
+int pyst_test_poisson(const float* d_lam, int64_t n, uint64_t seed,
+                      int32_t* d_out, void* stream) {
+  if (n <= 0) return PYST_OK;
+  if (!d_lam || !d_out) return PYST_EINVAL;
+  k_poisson<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+      d_lam, n, seed, d_out);
+  return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,104 @@
+"""Reaction networks of the benchmark workloads, built directly as engine
+models (no SBML file needed), plus the seeded generator of uneven synthetic
+networks for batched runs.
+
+* :func:`lotka_volterra` -- the network of ``examples/lotkaVoltera_sbml.xml``
+  (species x, y and a catalyst a fixed at 1): a + x -> a + 2x (k1 x a),
+  x + y -> 2y (k2 x y), y -> 0 (k3 y).
+* :func:`schlogl` -- the network of ``examples/schlogl_sbmlv2.xml`` with the
+  buffered species A, B folded into the rates: 2X -> 3X (c1/2 A X(X-1)),
+  3X -> 2X (c2/6 X(X-1)(X-2)), 0 -> X (c3 B), X -> 0 (c4 X).
+* :func:`telegraph` -- two-state gene expression (G_off, G_on, mRNA,
+  protein).
+* :func:`synthetic_networks` -- S ~ U[5,64], R ~ U[8,256] mass-action
+  networks with 0-2 reactants / products of stoichiometry 1-2, rate
+  constants log-uniform in [1e-3, 1e1], x0 ~ U{0..1000}, t_end log-uniform
+  in [1, 100].
+"""
+
+import numpy as np
+
+from .model import Model
+
+
+def _times(t_end, n):
+    return np.linspace(0, t_end, num=n).astype(np.float32)
+
+
+def lotka_volterra(k1=10.0, k2=0.01, k3=10.0, x0=(1000, 1000, 1), t_end=10.0,
+                   n_samples=100, out_species=(0, 1)):
+    pre = np.array([[1, 1, 0],
+                    [0, 1, 1],
+                    [1, 0, 0]])
+    post = np.array([[2, 0, 0],
+                     [0, 2, 0],
+                     [1, 0, 0]])
+    m = Model.mass_action(pre, post, [k1, k2, k3], x0, _times(t_end, n_samples),
+                          out_species, t_max=t_end)
+    m.name = 'lotka_volterra'
+    return m
+
+
+SCHLOGL_NOMINAL = dict(c1=3e-7, c2=1e-4, c3=1e-3, c4=3.5, A=1e5, B=2e5)
+
+
+def schlogl(c1=3e-7, c2=1e-4, c3=1e-3, c4=3.5, A=1e5, B=2e5, x0=250,
+            t_end=5.0, n_samples=200):
+    pre = np.array([[2, 3, 0, 1]])
+    post = np.array([[3, 2, 1, 0]])
+    # propensities c1/2 A X(X-1), c2/6 X(X-1)(X-2), c3 B, c4 X
+    rate = [c1 * A / 2.0, c2 / 6.0, c3 * B, c4]
+    m = Model(pre, pre, post - pre, rate, [x0], _times(t_end, n_samples), [0],
+              hor=[3], hor_type=[3], t_max=t_end)
+    m.name = 'schlogl'
+    return m
+
+
+TELEGRAPH_NOMINAL = (0.5, 0.2, 20.0, 1.0, 5.0, 0.1)
+
+
+def telegraph(k=TELEGRAPH_NOMINAL, t_end=50.0, n_samples=20,
+              out_species=(3,)):
+    """Species (G_off, G_on, mRNA, protein), x0 = (1, 0, 0, 0); reactions
+    off->on, on->off, on->on+mRNA, mRNA->0, mRNA->mRNA+protein,
+    protein->0."""
+    pre = np.array([[1, 0, 0, 0, 0, 0],
+                    [0, 1, 1, 0, 0, 0],
+                    [0, 0, 0, 1, 1, 0],
+                    [0, 0, 0, 0, 0, 1]])
+    post = np.array([[0, 1, 0, 0, 0, 0],
+                     [1, 0, 1, 0, 0, 0],
+                     [0, 0, 1, 0, 1, 0],
+                     [0, 0, 0, 0, 1, 0]])
+    m = Model.mass_action(pre, post, k, [1, 0, 0, 0], _times(t_end, n_samples),
+                          out_species, t_max=t_end)
+    m.name = 'telegraph'
+    return m
+
+
+def synthetic_networks(n_networks, seed=0, s_range=(5, 64), r_range=(8, 256),
+                       n_samples=50, k_range=(1e-3, 1e1), x0_max=1000,
+                       t_range=(1.0, 100.0)):
+    """Seeded uneven mass-action networks (list of :class:`Model`)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_networks):
+        S = int(rng.integers(s_range[0], s_range[1] + 1))
+        R = int(rng.integers(r_range[0], r_range[1] + 1))
+        pre = np.zeros((S, R), np.int64)
+        post = np.zeros((S, R), np.int64)
+        for j in range(R):
+            for mat in (pre, post):
+                n = int(rng.integers(0, 3))
+                sp = rng.choice(S, size=n, replace=False)
+                for i in sp:
+                    mat[i, j] = int(rng.integers(1, 3))
+        k = np.exp(rng.uniform(np.log(k_range[0]), np.log(k_range[1]), R))
+        x0 = rng.integers(0, x0_max + 1, S)
+        t_end = float(np.exp(rng.uniform(np.log(t_range[0]),
+                                         np.log(t_range[1]))))
+        m = Model.mass_action(pre, post, k, x0, _times(t_end, n_samples),
+                              np.arange(S), t_max=t_end)
+        m.name = 'synthetic'
+        out.append(m)
+    return out
