@@ -17,7 +17,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from .simulator import _mapping, _method, _torch
+from .simulator import DEFAULT_STEP_BUDGET, _mapping, _method, _torch
 
 
 def estimated_cost(model, method):
@@ -149,10 +149,12 @@ class Batch(object):
                                             dtype=torch.float64, device=dev)
 
     def run(self, seed=0, stream=None, ssa_fallback_steps=100,
-            max_leap_retries=63, step_budget=0, block_size=0):
+            max_leap_retries=63, step_budget=None, block_size=0):
         """Enqueue the whole batch on ``stream`` (one kernel launch)."""
         torch = _torch()
         L = _lib.lib()
+        if step_budget is None:
+            step_budget = DEFAULT_STEP_BUDGET
         o = self.out
         outs = _lib.Outputs(
             o['samples'].data_ptr(), 0,

@@ -78,11 +78,35 @@ def _compile(src, obj, defs, extra, verbose):
     return r.stdout + r.stderr
 
 
+STAMP = LIB + '.stamp'
+
+
+def source_hash():
+    """Content hash of every source, header and the compiler flags."""
+    import hashlib
+    h = hashlib.sha1(' '.join(NVCC_FLAGS).encode())
+    for f in sorted(set([os.path.join(CSRC, u[0]) for u in units()] +
+                        HEADERS)):
+        with open(f, 'rb') as fh:
+            h.update(os.path.basename(f).encode() + b'\0' + fh.read())
+    return h.hexdigest()
+
+
+def up_to_date():
+    if not os.path.exists(LIB) or not os.path.exists(STAMP):
+        return False
+    with open(STAMP) as f:
+        return f.read().strip() == source_hash()
+
+
 def build(force=False, verbose=False, extra=(), jobs=None):
-    """Compile stale objects in parallel and relink; return the .so path."""
-    srcs = [os.path.join(CSRC, u[0]) for u in units()] + HEADERS
-    if not force and not extra and not _stale(LIB, srcs):
-        return LIB  # objects may be absent (e.g. a copy without _build/)
+    """Compile stale objects in parallel and relink; return the .so path.
+
+    The library counts as current when its stamp file holds the content
+    hash of the sources (modification times are not trusted: copies of the
+    tree may not keep them)."""
+    if not force and not extra and up_to_date():
+        return LIB
     os.makedirs(BUILD, exist_ok=True)
     todo = []
     objs = []
@@ -105,6 +129,8 @@ def build(force=False, verbose=False, extra=(), jobs=None):
             print(' '.join(cmd), flush=True)
         subprocess.check_call(cmd)
         os.replace(LIB + '.tmp', LIB)
+    with open(STAMP, 'w') as f:
+        f.write(source_hash() + '\n')
     if extra and logs:
         print('\n'.join(l for l in logs if l.strip()))
     return LIB

@@ -27,6 +27,10 @@ METHODS = {'direct': _lib.METHOD_DIRECT, 'ssa': _lib.METHOD_DIRECT,
 MAPPINGS = {'auto': _lib.MAP_AUTO, 'thread': _lib.MAP_THREAD,
             'warp': _lib.MAP_WARP}
 
+# Steps (SSA events plus leaps) one trajectory may take before it stops with
+# status STEP_BUDGET; bounds the work of a run whose trajectories explode.
+DEFAULT_STEP_BUDGET = 100_000_000
+
 ERROR_STATUSES = (_lib.TRAJ_STEP_BUDGET, _lib.TRAJ_OVERFLOW,
                   _lib.TRAJ_LEAP_RETRY, _lib.TRAJ_SAMPLER, _lib.TRAJ_STAGING)
 
@@ -73,7 +77,7 @@ def device_blob(model, device):
 def simulate(model, n_traj, method='direct', seed=0, traj_id_base=0,
              mapping='auto', device=None, stream=None, status=True,
              events=True, seqhash=False, t_final=False, score=False,
-             step_budget=0, ssa_fallback_steps=100, max_leap_retries=63,
+             step_budget=DEFAULT_STEP_BUDGET, ssa_fallback_steps=100, max_leap_retries=63,
              block_size=0, out=None, d_blob=None):
     """Run ``n_traj`` trajectories of ``model`` (a :class:`Model`) on the GPU.
 
