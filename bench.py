@@ -187,8 +187,12 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default='schlogl_tau')
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--n-traj', type=int, default=0,
+                    help='override trajectories per GPU (profiling runs)')
     args = ap.parse_args()
     wl = workloads()[args.workload]
+    if args.n_traj:
+        wl['n'] = args.n_traj
     if args.impl == 'reference':
         return run_reference(args, wl)
 

@@ -80,7 +80,7 @@ class _OOut(C.Structure):
     _fields_ = [('samples', C.c_void_p), ('n', C.c_int64),
                 ('status', C.c_void_p), ('events', C.c_void_p),
                 ('seqhash', C.c_void_p), ('t_final', C.c_void_p),
-                ('score', C.c_void_p)]
+                ('score', C.c_void_p), ('steps', C.c_void_p)]
 
 
 _lib = None
@@ -196,11 +196,12 @@ def simulate(model, n_traj, method, seed=0, traj_id_base=0, warp=False,
         'seqhash': np.zeros(n_traj, dtype=np.uint64),
         't_final': np.zeros(n_traj, dtype=np.float64),
         'score': np.zeros((n_traj, R), dtype=np.float64),
+        'steps': np.zeros((n_traj, 2), dtype=np.int64),
     }
     oo = _OOut(res['samples'].ctypes.data, n_traj,
                res['status'].ctypes.data, res['events'].ctypes.data,
                res['seqhash'].ctypes.data, res['t_final'].ctypes.data,
-               res['score'].ctypes.data)
+               res['score'].ctypes.data, res['steps'].ctypes.data)
     rc = lib().oracle_simulate(C.byref(om), C.byref(ru), C.byref(oo), u0, u1,
                                int(threads))
     if rc != 0:

@@ -284,6 +284,7 @@ typedef struct {
   uint64_t* seqhash;
   double* t_final;
   double* score; /* [n][R] */
+  int64_t* steps; /* [n][2]: SSA steps, leaps (optional) */
 } oout;
 
 #define FNV_OFF 0xcbf29ce484222325ull
@@ -425,7 +426,7 @@ static void one_trajectory(const omodel* m, const float* rate32,
   }
   double t = 0.0;
   int f = 0;
-  int64_t events = 0, steps = 0;
+  int64_t events = 0, steps = 0, n_ssa = 0, n_leap = 0;
   uint64_t h = FNV_OFF;
   int status = 0, fill_state = 0;
   int64_t budget = ru->step_budget ? ru->step_budget : (1ll << 62);
@@ -483,6 +484,7 @@ static void one_trajectory(const omodel* m, const float* rate32,
         /* fall through to one SSA step with the same propensities */
       } else {
         steps++;
+        n_leap++;
         double a0c = total(ru, R, a, crit, partc, inclc);
         double tau2 = INFINITY;
         uint32_t wc[4] = {0, 0, 0, 0};
@@ -577,6 +579,7 @@ static void one_trajectory(const omodel* m, const float* rate32,
     }
     /* one direct-method step */
     steps++;
+    n_ssa++;
     uint32_t w[4];
     os_block(&rs, w);
     double tau = -oracle_log(u53(w[0], w[1])) / a0;
@@ -622,6 +625,10 @@ static void one_trajectory(const omodel* m, const float* rate32,
   if (o->events) o->events[u] = events;
   if (o->seqhash) o->seqhash[u] = h;
   if (o->t_final) o->t_final[u] = t;
+  if (o->steps) {
+    o->steps[2 * u] = n_ssa;
+    o->steps[2 * u + 1] = n_leap;
+  }
   if (o->score)
     for (int j = 0; j < R; ++j) o->score[u * R + j] = cnt[j] - integ[j];
 }

@@ -520,7 +520,7 @@ __device__ void run_warp(const ModelView& m, const WarpSmem& ws,
   const int j0 = min(R, lane * c), j1 = min(R, j0 + c);
   for (int i = lane; i < S; i += 32) ws.x[i] = m.x0(i);
   if (SCORE)
-    for (int j = lane; j < R; j += 32) score_acc[j] = 0.0;
+    for (int j = lane; j < 2 * R; j += 32) score_acc[j] = 0.0;
   __syncwarp();
   Stream rs = make_stream(ra.seed, traj_id);
   double t = 0.0;
