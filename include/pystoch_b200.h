@@ -136,13 +136,21 @@ int pyst_model_build(const pyst_model_desc* model, uint32_t* blob,
 
 /* Both single-model runs take the blob twice: `h_blob` (host copy; only
  * its header is read, to size the launch without a device round trip) and
- * `d_blob` (16-byte-aligned device copy the kernels stage). */
+ * `d_blob` (16-byte-aligned device copy the kernels stage).  `d_workspace`
+ * (8-byte aligned, >= pyst_run_workspace_size bytes) holds the trajectory
+ * work queue: launches size their grid to the GPU's resident capacity and a
+ * thread (or warp) whose trajectory ends takes the next unstarted one.  A
+ * workspace may be reused by consecutive calls on one stream, not by calls
+ * that overlap. */
+#define PYST_RUN_WORKSPACE_BYTES 256
+int pyst_run_workspace_size(const pyst_run_desc* run, size_t* bytes);
 
 /* Direct-method SSA (Gillespie), one trajectory per thread or per warp.
  * Replaces CuGillespie.run and the forced-SSA path of CuTauLeaping.run
  * (gillespie=1, P1_P2.py:68-74 + P3.py:71-151). */
 int pyst_ssa_direct_run(const uint32_t* h_blob, const uint32_t* d_blob,
                         const pyst_run_desc* run, const pyst_outputs* out,
+                        void* d_workspace, size_t workspace_bytes,
                         void* stream);
 
 /* Adaptive tau-leaping with critical reactions and SSA fallback, all
@@ -150,6 +158,7 @@ int pyst_ssa_direct_run(const uint32_t* h_blob, const uint32_t* d_blob,
  * cuTauLeaping.py:49-76 with kernel_P1_P2 and kernel_P3). */
 int pyst_tau_leap_run(const uint32_t* h_blob, const uint32_t* d_blob,
                       const pyst_run_desc* run, const pyst_outputs* out,
+                      void* d_workspace, size_t workspace_bytes,
                       void* stream);
 
 /* ---- batched persistent runs -------------------------------------------- */

@@ -204,7 +204,8 @@ int oracle_poisson(float lam, const opkey* pk) {
     int k = 0;
     while (u > F && k < 200) {
       k++;
-      p = (p * l) / (double)k;
+      double inv = 1.0 / (double)k;
+      p = (p * l) * inv;
       F = F + p;
     }
     return k;

@@ -37,6 +37,7 @@ MAX_SPECIES = 1024
 MAX_REACTIONS = 4096
 THREAD_MAX_REACTIONS = 32
 MAX_BLOB_WORDS = 12288
+RUN_WORKSPACE_BYTES = 256
 
 # header word indices (PYST_H_*)
 H_MAGIC, H_WORDS, H_S, H_R, H_KAPPA, H_ITA = 0, 1, 2, 3, 4, 5
@@ -89,10 +90,14 @@ SIGNATURES = {
     'pyst_model_blob_words': (C.c_int, [C.POINTER(ModelDesc),
                                         C.POINTER(C.c_int64)]),
     'pyst_model_build': (C.c_int, [C.POINTER(ModelDesc), _p, C.c_int64]),
+    'pyst_run_workspace_size': (C.c_int, [C.POINTER(RunDesc),
+                                          C.POINTER(C.c_size_t)]),
     'pyst_ssa_direct_run': (C.c_int, [_p, _p, C.POINTER(RunDesc),
-                                      C.POINTER(Outputs), _p]),
+                                      C.POINTER(Outputs), _p, C.c_size_t,
+                                      _p]),
     'pyst_tau_leap_run': (C.c_int, [_p, _p, C.POINTER(RunDesc),
-                                    C.POINTER(Outputs), _p]),
+                                    C.POINTER(Outputs), _p, C.c_size_t,
+                                    _p]),
     'pyst_batch_workspace_size': (C.c_int, [C.c_int64,
                                             C.POINTER(C.c_size_t)]),
     'pyst_batch_run': (C.c_int, [_p, _p, C.c_int64, C.POINTER(BatchLimits),

@@ -85,7 +85,8 @@ OutBase make_outbase(const pyst_outputs* out, int64_t n_traj) {
 }
 
 int single_run(const uint32_t* h_blob, const uint32_t* d_blob,
-               const pyst_run_desc* run, const pyst_outputs* out, void* stream,
+               const pyst_run_desc* run, const pyst_outputs* out,
+               void* d_workspace, size_t workspace_bytes, void* stream,
                int method) {
   HostModelInfo mi;
   int rc = read_header(h_blob, &mi);
@@ -97,9 +98,12 @@ int single_run(const uint32_t* h_blob, const uint32_t* d_blob,
   if (!out || !out->samples) return PYST_EINVAL;
   if (out->out_stride != 0 && out->out_stride < run->n_traj)
     return PYST_EINVAL;
+  if (!d_workspace || ((uintptr_t)d_workspace & 7)) return PYST_EINVAL;
+  if (workspace_bytes < PYST_RUN_WORKSPACE_BYTES) return PYST_EWORKSPACE;
   if (run->n_traj == 0) return PYST_OK;
   const RunArgs ra = make_args(run);
   const OutBase ob = make_outbase(out, run->n_traj);
+  unsigned long long* queue = (unsigned long long*)d_workspace;
   cudaStream_t st = (cudaStream_t)stream;
   const bool tau = method == PYST_METHOD_TAU_LEAP;
   const bool score = out->score != nullptr;
@@ -116,19 +120,23 @@ int single_run(const uint32_t* h_blob, const uint32_t* d_blob,
   if (mapping == PYST_MAP_THREAD) {
     if (tau)
       return score ? launch_plain_thread_11(mi.R, d_blob, mi, n, idb, ra, ob,
-                                            bs, st)
+                                            bs, queue, st)
                    : launch_plain_thread_10(mi.R, d_blob, mi, n, idb, ra, ob,
-                                            bs, st);
+                                            bs, queue, st);
     return score ? launch_plain_thread_01(mi.R, d_blob, mi, n, idb, ra, ob, bs,
-                                          st)
+                                          queue, st)
                  : launch_plain_thread_00(mi.R, d_blob, mi, n, idb, ra, ob, bs,
-                                          st);
+                                          queue, st);
   }
   if (tau)
-    return score ? launch_plain_warp_11(d_blob, mi, n, idb, ra, ob, bs, st)
-                 : launch_plain_warp_10(d_blob, mi, n, idb, ra, ob, bs, st);
-  return score ? launch_plain_warp_01(d_blob, mi, n, idb, ra, ob, bs, st)
-               : launch_plain_warp_00(d_blob, mi, n, idb, ra, ob, bs, st);
+    return score ? launch_plain_warp_11(d_blob, mi, n, idb, ra, ob, bs, queue,
+                                        st)
+                 : launch_plain_warp_10(d_blob, mi, n, idb, ra, ob, bs, queue,
+                                        st);
+  return score ? launch_plain_warp_01(d_blob, mi, n, idb, ra, ob, bs, queue,
+                                      st)
+               : launch_plain_warp_00(d_blob, mi, n, idb, ra, ob, bs, queue,
+                                      st);
 }
 
 }  // namespace
@@ -162,21 +170,31 @@ const char* pyst_traj_status_string(int code) {
   return "unknown trajectory status";
 }
 
+int pyst_run_workspace_size(const pyst_run_desc* run, size_t* bytes) {
+  if (!run || !bytes) return PYST_EINVAL;
+  *bytes = PYST_RUN_WORKSPACE_BYTES;
+  return PYST_OK;
+}
+
 int pyst_ssa_direct_run(const uint32_t* h_blob, const uint32_t* d_blob,
                         const pyst_run_desc* run, const pyst_outputs* out,
+                        void* d_workspace, size_t workspace_bytes,
                         void* stream) {
-  return single_run(h_blob, d_blob, run, out, stream, PYST_METHOD_DIRECT);
+  return single_run(h_blob, d_blob, run, out, d_workspace, workspace_bytes,
+                    stream, PYST_METHOD_DIRECT);
 }
 
 int pyst_tau_leap_run(const uint32_t* h_blob, const uint32_t* d_blob,
                       const pyst_run_desc* run, const pyst_outputs* out,
+                      void* d_workspace, size_t workspace_bytes,
                       void* stream) {
-  return single_run(h_blob, d_blob, run, out, stream, PYST_METHOD_TAU_LEAP);
+  return single_run(h_blob, d_blob, run, out, d_workspace, workspace_bytes,
+                    stream, PYST_METHOD_TAU_LEAP);
 }
 
 int pyst_batch_workspace_size(int64_t n_items, size_t* bytes) {
   if (!bytes || n_items < 0) return PYST_EINVAL;
-  *bytes = 256;  // the work-queue counter, padded
+  *bytes = PYST_RUN_WORKSPACE_BYTES;  // the work-queue counter, padded
   return PYST_OK;
 }
 
@@ -188,7 +206,7 @@ int pyst_batch_run(const uint32_t* d_blobs, const pyst_batch_item* d_items,
     return PYST_EINVAL;
   if (((uintptr_t)d_blobs & 15) || n_items < 0) return PYST_EINVAL;
   if (!d_workspace || ((uintptr_t)d_workspace & 7)) return PYST_EINVAL;
-  if (workspace_bytes < 256) return PYST_EWORKSPACE;
+  if (workspace_bytes < PYST_RUN_WORKSPACE_BYTES) return PYST_EWORKSPACE;
   if (lim->max_blob_words <= 0 || (lim->max_blob_words & 3) ||
       lim->max_blob_words > PYST_MAX_BLOB_WORDS || lim->max_species < 1 ||
       lim->max_reactions < 1 || lim->max_species > PYST_MAX_SPECIES ||

@@ -18,7 +18,8 @@ namespace {
 template <int MAXR, bool TAU, bool SCORE>
 __global__ void __launch_bounds__(128)
     k_plain_thread(const uint32_t* __restrict__ gblob, int blob_words,
-                   int64_t n_traj, uint64_t id_base, RunArgs ra, OutBase ob) {
+                   int64_t n_traj, uint64_t id_base, RunArgs ra, OutBase ob,
+                   unsigned long long* queue) {
   extern __shared__ __align__(16) unsigned char smem[];
   uint32_t* sblob = (uint32_t*)smem;
   uint64_t* bar = (uint64_t*)(smem + (size_t)blob_words * 4);
@@ -30,30 +31,45 @@ __global__ void __launch_bounds__(128)
   __syncthreads();
   const bool ok = stage_blob(sblob, gblob, blob_words, bar, 0);
   const int bs = blockDim.x;
-  const int64_t u = blockIdx.x * (int64_t)bs + threadIdx.x;
+  const int64_t nthreads = (int64_t)gridDim.x * bs;
+  // first trajectory by thread index, later ones from the shared queue, so
+  // a thread whose trajectory ends early takes the next unstarted one
+  int64_t u = blockIdx.x * (int64_t)bs + threadIdx.x;
   if (!ok) {
     mbar_wait(bar, 0);  // let a late copy land before the block exits
-    if (u < n_traj) mark_staging_failure(ob, u);
+    while (u < n_traj) {
+      mark_staging_failure(ob, u);
+      u = nthreads + (int64_t)atomicAdd(queue, 1ull);
+    }
     return;
   }
-  if (u >= n_traj) return;
   ModelView m;
   m.load(sblob);
   int32_t* xcol = xbase + threadIdx.x;
   int64_t* slot = (int64_t*)(xbase + (size_t)m.S * bs) + threadIdx.x;
-  const TrajOut o = ob.at(0, u, 0, 0, ob.stride, m.R);
-  run_thread<MAXR, TAU, SCORE>(m, xcol, slot, bs, ra, id_base + (uint64_t)u,
-                               o);
+  while (u < n_traj) {
+    const TrajOut o = ob.at(0, u, 0, 0, ob.stride, m.R);
+    run_thread<MAXR, TAU, SCORE>(m, xcol, slot, bs, ra,
+                                 id_base + (uint64_t)u, o);
+    u = nthreads + (int64_t)atomicAdd(queue, 1ull);
+  }
 }
 
 template <int MR>
 int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
                uint64_t id_base, const RunArgs& ra, const OutBase& ob, int bs,
-               cudaStream_t st, size_t smem, int64_t grid) {
+               cudaStream_t st, size_t smem, unsigned long long* queue) {
   auto kf = k_plain_thread<MR, (bool)PYST_TAU, (bool)PYST_SCORE>;
   const int rc = set_smem(kf, smem);
   if (rc) return rc;
-  kf<<<(unsigned)grid, bs, smem, st>>>(d_blob, mi.words, n, id_base, ra, ob);
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf, bs, smem);
+  if (per_sm < 1) per_sm = 1;
+  int64_t grid = (n + bs - 1) / bs;
+  const int64_t cap = (int64_t)num_sms() * per_sm;
+  if (grid > cap) grid = cap;
+  kf<<<(unsigned)grid, bs, smem, st>>>(d_blob, mi.words, n, id_base, ra, ob,
+                                       queue);
   return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
 }
 
@@ -62,16 +78,22 @@ int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
 int PYST_CAT(launch_plain_thread_, PYST_TAU, PYST_SCORE)(
     int maxr, const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
     uint64_t id_base, const RunArgs& ra, const OutBase& ob, int bs,
-    cudaStream_t st) {
+    unsigned long long* queue, cudaStream_t st) {
   const size_t smem =
       (size_t)mi.words * 4 + 16 + (size_t)bs * mi.S * (PYST_TAU ? 12 : 4);
   if (smem > kMaxDynSmem) return PYST_EUNSUPPORTED;
-  const int64_t grid = (n + bs - 1) / bs;
-  if (grid == 0) return PYST_OK;
-  if (maxr <= 4) return launch_one<4>(d_blob, mi, n, id_base, ra, ob, bs, st, smem, grid);
-  if (maxr <= 8) return launch_one<8>(d_blob, mi, n, id_base, ra, ob, bs, st, smem, grid);
-  if (maxr <= 16) return launch_one<16>(d_blob, mi, n, id_base, ra, ob, bs, st, smem, grid);
-  return launch_one<32>(d_blob, mi, n, id_base, ra, ob, bs, st, smem, grid);
+  if (n <= 0) return PYST_OK;
+  if (cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st) !=
+      cudaSuccess)
+    return PYST_ECUDA;
+  if (maxr <= 4)
+    return launch_one<4>(d_blob, mi, n, id_base, ra, ob, bs, st, smem, queue);
+  if (maxr <= 8)
+    return launch_one<8>(d_blob, mi, n, id_base, ra, ob, bs, st, smem, queue);
+  if (maxr <= 16)
+    return launch_one<16>(d_blob, mi, n, id_base, ra, ob, bs, st, smem,
+                          queue);
+  return launch_one<32>(d_blob, mi, n, id_base, ra, ob, bs, st, smem, queue);
 }
 
 }  // namespace pyst

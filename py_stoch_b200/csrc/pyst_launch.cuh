@@ -76,7 +76,8 @@ int num_sms();
   int launch_plain_thread_##T##SC(int maxr, const uint32_t* d_blob,          \
                                   const HostModelInfo& mi, int64_t n,        \
                                   uint64_t id_base, const RunArgs& ra,       \
-                                  const OutBase& ob, int bs, cudaStream_t st);
+                                  const OutBase& ob, int bs,                 \
+                                  unsigned long long* queue, cudaStream_t st);
 PYST_DECL_THREAD(0, 0)
 PYST_DECL_THREAD(0, 1)
 PYST_DECL_THREAD(1, 0)
@@ -87,7 +88,8 @@ PYST_DECL_THREAD(1, 1)
   int launch_plain_warp_##T##SC(const uint32_t* d_blob,                      \
                                 const HostModelInfo& mi, int64_t n,          \
                                 uint64_t id_base, const RunArgs& ra,         \
-                                const OutBase& ob, int bs, cudaStream_t st);
+                                const OutBase& ob, int bs,                   \
+                                unsigned long long* queue, cudaStream_t st);
 PYST_DECL_WARP(0, 0)
 PYST_DECL_WARP(0, 1)
 PYST_DECL_WARP(1, 0)

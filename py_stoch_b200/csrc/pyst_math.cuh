@@ -201,8 +201,9 @@ __device__ __forceinline__ uint4 pblock(const PoissonKey& pk, uint32_t blk) {
 
 // Poisson(lam) with lam in FP32.  Returns K >= 0; -1 if the rejection
 // loop ran out of iterations; -2 if lam is beyond the supported range.
-// Draws nothing when lam <= 0.
-__device__ __forceinline__ int poisson(float lam, const PoissonKey& pk) {
+// Draws nothing when lam <= 0.  Kept out of line: a leap calls it once per
+// reaction, and one shared copy keeps the instruction footprint small.
+static __device__ __noinline__ int poisson(float lam, const PoissonKey& pk) {
   if (!(lam > 0.0f)) return 0;
   if (!(lam <= PYST_POISSON_MAX_LAMBDA)) return -2;
   if (lam < 10.0f) {
@@ -214,7 +215,8 @@ __device__ __forceinline__ int poisson(float lam, const PoissonKey& pk) {
     int k = 0;
     while (u > F && k < PYST_INVERSION_MAX_K) {
       k++;
-      p = __ddiv_rn(__dmul_rn(p, l), (double)k);
+      // p_k = p_{k-1} * lam * (1/k); 1/k correctly rounded
+      p = __dmul_rn(__dmul_rn(p, l), __drcp_rn((double)k));
       F = __dadd_rn(F, p);
     }
     return k;

@@ -124,13 +124,17 @@ def simulate(model, n_traj, method='direct', seed=0, traj_id_base=0,
     if stream is None:
         stream = torch.cuda.current_stream(device)
     sptr = C.c_void_p(stream.cuda_stream)
+    ws = out.get('workspace')
+    if ws is None:
+        ws = torch.empty(_lib.RUN_WORKSPACE_BYTES, dtype=torch.uint8,
+                         device=device)
     fn = (L.pyst_ssa_direct_run if meth == _lib.METHOD_DIRECT
           else L.pyst_tau_leap_run)
     _lib.check(fn(h_blob.ctypes.data, d_blob.data_ptr(), C.byref(r),
-                  C.byref(o), sptr),
+                  C.byref(o), ws.data_ptr(), ws.numel(), sptr),
                'pyst_ssa_direct_run' if meth == _lib.METHOD_DIRECT
                else 'pyst_tau_leap_run')
-    res['_keepalive'] = (d_blob, h_blob)
+    res['_keepalive'] = (d_blob, h_blob, ws)
     return res
 
 

@@ -1,0 +1,132 @@
+"""The C ABI library: loads without a GPU, exports every function the public
+headers declare, and rejects bad arguments before any CUDA call."""
+
+import ctypes as C
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+from py_stoch_b200 import _lib, networks
+
+INCLUDE = os.path.join(os.path.dirname(os.path.dirname(
+    os.path.abspath(__file__))), 'include')
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(INCLUDE, '*.h')):
+        text = open(h).read()
+        text = re.sub(r'/\*.*?\*/', '', text, flags=re.S)
+        for m in re.finditer(r'^\s*(?:const\s+)?\w+\s*\*?\s*(pyst_\w+)\s*\(',
+                             text, flags=re.M):
+            names.add(m.group(1))
+    return names
+
+
+def test_exports_every_declared_symbol(built_lib):
+    names = declared_functions()
+    assert 'pyst_tau_leap_run' in names and 'pyst_batch_run' in names
+    for n in names:
+        assert hasattr(built_lib, n), n
+        assert n in _lib.SIGNATURES, n
+
+
+def test_version_and_strings(built_lib):
+    assert built_lib.pyst_abi_version() == 1
+    for code in range(6):
+        assert built_lib.pyst_status_string(code)
+    for code in range(7):
+        assert built_lib.pyst_traj_status_string(code)
+
+
+def _run_args():
+    r = _lib.RunDesc(16, 0, 1, 0, 0, 100, 63, 0, 0, 0)
+    o = _lib.Outputs(0, 0, 0, 0, 0, 0, 0)
+    return r, o
+
+
+def test_run_rejects_bad_arguments(built_lib):
+    L = built_lib
+    m = networks.lotka_volterra()
+    blob = m.blob()
+    r, o = _run_args()
+    # null host blob
+    assert L.pyst_ssa_direct_run(None, 16, C.byref(r), C.byref(o), 8, 256,
+                                 None) == _lib.PYST_EINVAL
+    # corrupt magic
+    bad = blob.copy()
+    bad[0] = 0
+    assert L.pyst_ssa_direct_run(bad.ctypes.data, 16, C.byref(r), C.byref(o),
+                                 8, 256, None) == _lib.PYST_EINVAL
+    # misaligned device blob pointer, null samples, missing workspace
+    assert L.pyst_ssa_direct_run(blob.ctypes.data, 17, C.byref(r),
+                                 C.byref(o), 8, 256,
+                                 None) == _lib.PYST_EINVAL
+    o.samples = 4096
+    assert L.pyst_ssa_direct_run(blob.ctypes.data, 16, C.byref(r),
+                                 C.byref(o), None, 256,
+                                 None) == _lib.PYST_EINVAL
+    assert L.pyst_ssa_direct_run(blob.ctypes.data, 16, C.byref(r),
+                                 C.byref(o), 8, 16,
+                                 None) == _lib.PYST_EWORKSPACE
+    # method mismatch and invalid tau parameters
+    assert L.pyst_tau_leap_run(blob.ctypes.data, 16, C.byref(r), C.byref(o),
+                               8, 256, None) == _lib.PYST_EINVAL
+    r.method = 1
+    r.max_leap_retries = 64
+    assert L.pyst_tau_leap_run(blob.ctypes.data, 16, C.byref(r), C.byref(o),
+                               8, 256, None) == _lib.PYST_EINVAL
+    r.max_leap_retries = 63
+    r.ssa_fallback_steps = 0
+    assert L.pyst_tau_leap_run(blob.ctypes.data, 16, C.byref(r), C.byref(o),
+                               8, 256, None) == _lib.PYST_EINVAL
+    r.ssa_fallback_steps = 100
+    r.block_size = 100
+    assert L.pyst_tau_leap_run(blob.ctypes.data, 16, C.byref(r), C.byref(o),
+                               8, 256, None) == _lib.PYST_EINVAL
+    # thread mapping on a model with too many reactions
+    big = networks.synthetic_networks(1, seed=1, r_range=(100, 100))[0]
+    r.block_size = 0
+    r.mapping = _lib.MAP_THREAD
+    assert L.pyst_tau_leap_run(big.blob().ctypes.data, 16, C.byref(r),
+                               C.byref(o), 8, 256,
+                               None) == _lib.PYST_EUNSUPPORTED
+    ws = C.c_size_t(0)
+    assert L.pyst_run_workspace_size(C.byref(r), C.byref(ws)) == 0
+    assert ws.value == _lib.RUN_WORKSPACE_BYTES
+
+
+def test_batch_and_backward_reject(built_lib):
+    L = built_lib
+    r, o = _run_args()
+    lim = _lib.BatchLimits(0, 1, 1, 0)
+    assert L.pyst_batch_run(None, None, 1, C.byref(lim), C.byref(r),
+                            C.byref(o), None, 0, None) == _lib.PYST_EINVAL
+    o.samples = 4096
+    assert L.pyst_batch_run(16, 16, 1, C.byref(lim), C.byref(r), C.byref(o),
+                            8, 256, None) == _lib.PYST_EUNSUPPORTED
+    lim = _lib.BatchLimits(64, 1, 1, 0)
+    assert L.pyst_batch_run(16, 16, 1, C.byref(lim), C.byref(r), C.byref(o),
+                            8, 8, None) == _lib.PYST_EWORKSPACE
+    ws = C.c_size_t(0)
+    assert L.pyst_score_backward_workspace_size(1000, 6, C.byref(ws)) == 0
+    assert ws.value == 4 * 6 * 8
+    assert L.pyst_score_backward(None, None, 10, 1, 1, 1, None, None, None,
+                                 None, None, None, 0,
+                                 None) == _lib.PYST_EINVAL
+    assert L.pyst_score_backward(8, 8, 10, 1, 1, 1, 8, None, 8, 8, 8, 8,
+                                 4096, None) == _lib.PYST_EINVAL
+
+
+def test_blob_size_query_matches_build(built_lib):
+    m = networks.schlogl()
+    d = m.desc()
+    n = C.c_int64(0)
+    assert built_lib.pyst_model_blob_words(C.byref(d), C.byref(n)) == 0
+    buf = np.zeros(n.value - 4, np.uint32)
+    assert built_lib.pyst_model_build(C.byref(d), buf.ctypes.data,
+                                      buf.size) == _lib.PYST_EINVAL
+    assert len(m.blob()) == n.value
