@@ -86,16 +86,31 @@ class _OOut(C.Structure):
 _lib = None
 
 
+CFLAGS = ['-O2', '-fPIC', '-ffp-contract=off', '-fno-fast-math', '-std=c11',
+          '-shared']
+STAMP = LIB + '.stamp'
+
+
+def _source_hash():
+    import hashlib
+    with open(SRC, 'rb') as f:
+        return hashlib.sha1(' '.join(CFLAGS).encode() + f.read()).hexdigest()
+
+
 def build(force=False):
-    """Compile liboracle.so if it is missing or older than its source."""
-    if (not force and os.path.exists(LIB)
-            and os.path.getmtime(LIB) >= os.path.getmtime(SRC)):
-        return LIB
+    """Compile liboracle.so unless its stamp holds the source's content
+    hash (modification times are not trusted across copies of the tree)."""
+    h = _source_hash()
+    if not force and os.path.exists(LIB) and os.path.exists(STAMP):
+        with open(STAMP) as f:
+            if f.read().strip() == h:
+                return LIB
     cc = os.environ.get('CC', 'gcc')
-    subprocess.check_call([cc, '-O2', '-fPIC', '-ffp-contract=off',
-                           '-fno-fast-math', '-std=c11', '-shared', '-o',
-                           LIB + '.tmp', SRC, '-lm', '-lpthread'])
+    subprocess.check_call([cc] + CFLAGS + ['-o', LIB + '.tmp', SRC, '-lm',
+                                           '-lpthread'])
     os.replace(LIB + '.tmp', LIB)
+    with open(STAMP, 'w') as f:
+        f.write(h + '\n')
     return LIB
 
 

@@ -9,7 +9,10 @@
 #include "pyst_launch.cuh"
 
 namespace pyst {
-namespace {
+// nvcc gives template functions of an anonymous namespace weak external
+// linkage on the host side, so the flavours built from this file would be
+// merged at link time; a per-flavour namespace keeps them apart.
+namespace PYST_CAT(batch_flavour_, PYST_SCORE, ) {
 
 template <bool SCORE>
 __global__ void __launch_bounds__(128)
@@ -80,7 +83,8 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-}  // namespace
+}  // namespace (flavour)
+using namespace PYST_CAT(batch_flavour_, PYST_SCORE, );
 
 int PYST_CAT(launch_batch_, PYST_SCORE, )(
     const uint32_t* d_blobs, const pyst_batch_item* d_items, int64_t n_items,

@@ -13,7 +13,10 @@
 #endif
 
 namespace pyst {
-namespace {
+// nvcc gives template functions of an anonymous namespace weak external
+// linkage on the host side, so the flavours built from this file would be
+// merged at link time; a per-flavour namespace keeps them apart.
+namespace PYST_CAT(thread_flavour_, PYST_TAU, PYST_SCORE) {
 
 template <int MAXR, bool TAU, bool SCORE>
 __global__ void __launch_bounds__(128)
@@ -73,7 +76,8 @@ int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
   return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
 }
 
-}  // namespace
+}  // namespace (flavour)
+using namespace PYST_CAT(thread_flavour_, PYST_TAU, PYST_SCORE);
 
 int PYST_CAT(launch_plain_thread_, PYST_TAU, PYST_SCORE)(
     int maxr, const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,

@@ -4,7 +4,10 @@
 #include "pyst_launch.cuh"
 
 namespace pyst {
-namespace {
+// nvcc gives template functions of an anonymous namespace weak external
+// linkage on the host side, so the flavours built from this file would be
+// merged at link time; a per-flavour namespace keeps them apart.
+namespace PYST_CAT(warp_flavour_, PYST_TAU, PYST_SCORE) {
 
 template <bool TAU, bool SCORE>
 __global__ void __launch_bounds__(128)
@@ -50,7 +53,8 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-}  // namespace
+}  // namespace (flavour)
+using namespace PYST_CAT(warp_flavour_, PYST_TAU, PYST_SCORE);
 
 int PYST_CAT(launch_plain_warp_, PYST_TAU, PYST_SCORE)(
     const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
