@@ -60,6 +60,11 @@ enum {
 enum { PYST_METHOD_DIRECT = 0, PYST_METHOD_TAU_LEAP = 1 };
 enum { PYST_MAP_AUTO = 0, PYST_MAP_THREAD = 1, PYST_MAP_WARP = 2 };
 
+/* pyst_run_desc.flags bits.  PYST_FLAG_UNSORTED: run thread-mapped
+ * tau-leaping with the simple one-trajectory-per-thread loop instead of the
+ * default mode-sorted block scheduler (same results, slower). */
+enum { PYST_FLAG_UNSORTED = 1 };
+
 /* Limits of this build. */
 #define PYST_MAX_SPECIES 1024
 #define PYST_MAX_REACTIONS 4096
@@ -108,7 +113,7 @@ typedef struct pyst_run_desc {
   int32_t max_leap_retries;    /* tau halvings before giving up (64)        */
   int64_t step_budget;         /* max steps per trajectory (0 = 2^62)       */
   int32_t block_size;          /* 0 = library default                       */
-  int32_t flags;               /* reserved, 0                               */
+  int32_t flags;               /* PYST_FLAG_* bits                          */
 } pyst_run_desc;
 
 /* Outputs (device pointers).  `samples` is required, the rest optional. */

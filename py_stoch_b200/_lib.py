@@ -32,6 +32,7 @@ METHOD_TAU_LEAP = 1
 MAP_AUTO = 0
 MAP_THREAD = 1
 MAP_WARP = 2
+FLAG_UNSORTED = 1
 
 MAX_SPECIES = 1024
 MAX_REACTIONS = 4096

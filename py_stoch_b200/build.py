@@ -6,7 +6,7 @@ The library links these objects with the static CUDA runtime, so it loads
 on machines without a GPU (only the run calls need one):
 
 * pyst_k_thread.cu, pyst_k_warp.cu  x (PYST_TAU, PYST_SCORE) in {0,1}^2
-* pyst_k_batch.cu                   x PYST_SCORE in {0,1}
+* pyst_k_batch.cu, pyst_k_sorted.cu x PYST_SCORE in {0,1}
 * pyst_k_misc.cu (gradient reduction, test hooks), pyst_capi.cu (C ABI)
 * pyst_pack.cpp (host-only model packer)
 
@@ -46,6 +46,8 @@ def units():
                             ['-DPYST_TAU=%d' % t, '-DPYST_SCORE=%d' % s]))
     for s in (0, 1):
         out.append(('pyst_k_batch.cu', 'pyst_k_batch_s%d.o' % s,
+                    ['-DPYST_SCORE=%d' % s]))
+        out.append(('pyst_k_sorted.cu', 'pyst_k_sorted_s%d.o' % s,
                     ['-DPYST_SCORE=%d' % s]))
     out.append(('pyst_k_misc.cu', 'pyst_k_misc.o', []))
     out.append(('pyst_capi.cu', 'pyst_capi.o', []))

@@ -30,6 +30,11 @@ using namespace pyst;
 
 namespace {
 
+// Round lengths of the mode-sorted tau-leaping kernel: SSA steps and leaps
+// a trajectory advances between two regroupings of its block.
+constexpr int kSortedCapSsa = 256;
+constexpr int kSortedCapLeap = 32;
+
 int read_header(const uint32_t* h, HostModelInfo* mi) {
   if (!h) return PYST_EINVAL;
   if (h[PYST_H_MAGIC] != PYST_BLOB_MAGIC) return PYST_EINVAL;
@@ -117,6 +122,12 @@ int single_run(const uint32_t* h_blob, const uint32_t* d_blob,
     return PYST_EUNSUPPORTED;
   const uint64_t idb = (uint64_t)run->traj_id_base;
   const int64_t n = run->n_traj;
+  if (mapping == PYST_MAP_THREAD && tau &&
+      !(run->flags & PYST_FLAG_UNSORTED))
+    return score ? launch_tau_sorted_1(mi.R, d_blob, mi, n, idb, ra, ob, queue,
+                                       kSortedCapSsa, kSortedCapLeap, st)
+                 : launch_tau_sorted_0(mi.R, d_blob, mi, n, idb, ra, ob, queue,
+                                       kSortedCapSsa, kSortedCapLeap, st);
   if (mapping == PYST_MAP_THREAD) {
     if (tau)
       return score ? launch_plain_thread_11(mi.R, d_blob, mi, n, idb, ra, ob,

@@ -129,38 +129,81 @@ __device__ __forceinline__ void store_sample(const TrajOut& o, int ita, int k,
 // ===================================================================
 // one trajectory per thread
 // ===================================================================
+// Everything a thread-mapped trajectory carries between steps, apart from
+// its species counts (shared-memory column) and score accumulators.  Split
+// out so a block can park a trajectory between scheduling rounds.
+struct TState {
+  double t;
+  uint64_t n;        // Philox block index of the main stream
+  int64_t events;
+  int64_t steps;
+  uint64_t h;        // firing-sequence hash
+  int32_t f;         // next sample index
+  uint32_t leap_q;   // leaps taken (Poisson stream counter)
+  int32_t ssa_left;  // SSA steps left in the current fallback round
+  int32_t flags;     // TS_* bits, status in bits 8..15
+};
+
+enum {
+  TS_SSA = 1,        // in an SSA fallback round (else DECIDE next)
+  TS_LEAPGRP = 2,    // last DECIDE chose to leap
+  TS_DONE = 4,       // trajectory finished
+  TS_FILL = 8        // absorbed: remaining samples take the final state
+};
+
+__device__ __forceinline__ int ts_status(const TState& s) {
+  return (s.flags >> 8) & 0xFF;
+}
+
+template <bool TAU>
+__device__ __forceinline__ void thread_init(const ModelView& m, int32_t* xcol,
+                                            int bs, TState& s) {
+  for (int i = 0; i < m.S; ++i) xcol[(int64_t)i * bs] = m.x0(i);
+  s.t = 0.0;
+  s.n = 0;
+  s.events = 0;
+  s.steps = 0;
+  s.h = PYST_FNV_OFFSET;
+  s.f = 0;
+  s.leap_q = 0;
+  s.ssa_left = 0;
+  s.flags = TAU ? TS_LEAPGRP : TS_SSA;
+}
+
+// Advance one trajectory.  Returns when it finishes, or -- for block
+// scheduling -- when it has taken cap_ssa SSA steps or cap_leap leaps in
+// this call, or when a DECIDE picks the other mode than the one the call
+// started in (stop_on_switch).  With unbounded caps this is the whole
+// trajectory.
 template <int MAXR, bool TAU, bool SCORE>
-__device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
-                           int bs, const RunArgs& ra, uint64_t traj_id,
-                           const TrajOut& o) {
+__device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
+                             int bs, const RunArgs& ra, uint64_t traj_id,
+                             TState& st, double* integ, int* cnt,
+                             const TrajOut& o, int cap_ssa, int cap_leap,
+                             bool stop_on_switch) {
   const int S = m.S, R = m.R, ita = m.ita, kappa = m.kappa;
 #define XV(i) xcol[(int64_t)(i) * bs]
 #define SL(i) slot[(int64_t)(i) * bs]
-  for (int i = 0; i < S; ++i) XV(i) = m.x0(i);
   Stream rs = make_stream(ra.seed, traj_id);
-  double t = 0.0;
-  int f = 0;
-  int64_t events = 0, steps = 0;
-  uint64_t h = PYST_FNV_OFFSET;
+  rs.n = st.n;
+  double t = st.t;
+  int f = st.f;
+  int64_t events = st.events, steps = st.steps;
+  uint64_t h = st.h;
   int status = PYST_TRAJ_DONE;
-  bool fill_state = false;
+  bool fill_state = false, done = false;
   const int64_t budget = ra.step_budget;
   const double t_end = m.time(ita - 1);
-  double integ[SCORE ? MAXR : 1];
-  int cnt[SCORE ? MAXR : 1];
-  if (SCORE) {
-#pragma unroll
-    for (int j = 0; j < MAXR; ++j) {
-      integ[j] = 0.0;
-      cnt[j] = 0;
-    }
-  }
-  bool ssa_mode = !TAU;
-  int ssa_left = 0;
-  uint32_t leap_q = 0;
+  bool ssa_mode = (st.flags & TS_SSA) != 0;
+  const bool group_leap = (st.flags & TS_LEAPGRP) != 0;
+  bool leap_grp = group_leap;
+  int ssa_left = st.ssa_left;
+  uint32_t leap_q = st.leap_q;
+  int n_ssa = 0, n_leap = 0;
   auto xget = [&](int i) { return XV(i); };
 
   while (true) {
+    if (n_ssa >= cap_ssa || n_leap >= cap_leap) break;
     float a[MAXR];
     double a0 = 0.0;
 #pragma unroll
@@ -172,10 +215,12 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
     if (a0 == 0.0) {
       status = PYST_TRAJ_ABSORBED;
       fill_state = true;
+      done = true;
       break;
     }
     if (steps >= budget) {
       status = PYST_TRAJ_STEP_BUDGET;
+      done = true;
       break;
     }
     if (TAU && !ssa_mode) {
@@ -219,10 +264,15 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
       if ((double)tau1 < __ddiv_rn(10.0, a0)) {
         ssa_mode = true;
         ssa_left = ra.ssa_fallback_steps;
+        leap_grp = false;
+        if (stop_on_switch && group_leap) break;  // regroup before stepping
         // fall through to the SSA step below with the same propensities
       } else {
+        leap_grp = true;
+        if (stop_on_switch && !group_leap) break;
         // ---------------- leap ---------------------------------------
         steps++;
+        n_leap++;
         double a0c = 0.0;
 #pragma unroll
         for (int j = 0; j < MAXR; ++j) {
@@ -310,7 +360,10 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
             break;
           }
         }
-        if (!ok) break;
+        if (!ok) {
+          done = true;
+          break;
+        }
         leap_q++;
         const double tn = __dadd_rn(t, tau);
         int64_t fired = 0;
@@ -325,7 +378,6 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
             integ[j] = __dadd_rn(integ[j], __dmul_rn((double)a[j], tau));
           }
         }
-        bool done = false;
         while (tn >= m.time(f)) {
           const double frac = __ddiv_rn(__dsub_rn(m.time(f), t), tau);
           for (int k = 0; k < kappa; ++k) {
@@ -348,6 +400,7 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
     }
     // ------------------------ one direct-method step -------------------
     steps++;
+    n_ssa++;
     const uint4 w = next_block(rs);
     const double tau = __ddiv_rn(-pyst_log(u53(w.x, w.y)), a0);
     const double r = __dmul_rn(u53(w.z, w.w), a0);
@@ -378,7 +431,6 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
         integ[j] = __dadd_rn(integ[j], __dmul_rn((double)a[j], dt));
       }
     }
-    bool done = false;
     while (tn >= m.time(f)) {
       for (int k = 0; k < kappa; ++k) store_sample(o, ita, k, f, XV(m.out(k)));
       f++;
@@ -401,6 +453,7 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
       }
       if (over) {
         status = PYST_TRAJ_OVERFLOW;
+        done = true;
         break;
       }
     }
@@ -414,14 +467,37 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
       if (--ssa_left <= 0) ssa_mode = false;
     }
   }
-  // remaining samples: state after absorption, -1 after an error
-  for (; f < ita; ++f)
+  st.t = t;
+  st.n = rs.n;
+  st.events = events;
+  st.steps = steps;
+  st.h = h;
+  st.f = f;
+  st.leap_q = leap_q;
+  st.ssa_left = ssa_left;
+  st.flags = (ssa_mode ? TS_SSA : 0) | (leap_grp ? TS_LEAPGRP : 0) |
+             (done ? TS_DONE : 0) | (fill_state ? TS_FILL : 0) |
+             (status << 8);
+#undef XV
+#undef SL
+}
+
+// Write the remaining samples (state after absorption, -1 after an error)
+// and the per-trajectory outputs of a finished trajectory.
+template <int MAXR, bool SCORE>
+__device__ void thread_finish(const ModelView& m, const int32_t* xcol, int bs,
+                              const TState& st, const double* integ,
+                              const int* cnt, const TrajOut& o) {
+  const int ita = m.ita, kappa = m.kappa, R = m.R;
+  const bool fill_state = (st.flags & TS_FILL) != 0;
+  for (int f = st.f; f < ita; ++f)
     for (int k = 0; k < kappa; ++k)
-      store_sample(o, ita, k, f, fill_state ? XV(m.out(k)) : -1);
-  if (o.status) *o.status = (uint8_t)status;
-  if (o.events) *o.events = events;
-  if (o.seqhash) *o.seqhash = h;
-  if (o.t_final) *o.t_final = t;
+      store_sample(o, ita, k, f,
+                   fill_state ? xcol[(int64_t)m.out(k) * bs] : -1);
+  if (o.status) *o.status = (uint8_t)ts_status(st);
+  if (o.events) *o.events = st.events;
+  if (o.seqhash) *o.seqhash = st.h;
+  if (o.t_final) *o.t_final = st.t;
   if (SCORE && o.score) {
 #pragma unroll
     for (int j = 0; j < MAXR; ++j) {
@@ -429,8 +505,25 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
       o.score[j] = __dsub_rn((double)cnt[j], integ[j]);
     }
   }
-#undef XV
-#undef SL
+}
+
+// One whole trajectory by the calling thread.
+template <int MAXR, bool TAU, bool SCORE>
+__device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
+                           int bs, const RunArgs& ra, uint64_t traj_id,
+                           const TrajOut& o) {
+  TState st;
+  thread_init<TAU>(m, xcol, bs, st);
+  double integ[SCORE ? MAXR : 1];
+  int cnt[SCORE ? MAXR : 1];
+#pragma unroll
+  for (int j = 0; j < (SCORE ? MAXR : 1); ++j) {
+    integ[j] = 0.0;
+    cnt[j] = 0;
+  }
+  thread_round<MAXR, TAU, SCORE>(m, xcol, slot, bs, ra, traj_id, st, integ,
+                                 cnt, o, 0x7fffffff, 0x7fffffff, false);
+  thread_finish<MAXR, SCORE>(m, xcol, bs, st, integ, cnt, o);
 }
 
 // ===================================================================

@@ -106,6 +106,16 @@ PYST_DECL_BATCH(0)
 PYST_DECL_BATCH(1)
 #undef PYST_DECL_BATCH
 
+#define PYST_DECL_SORTED(SC)                                                 \
+  int launch_tau_sorted_##SC(int maxr, const uint32_t* d_blob,               \
+                             const HostModelInfo& mi, int64_t n,             \
+                             uint64_t id_base, const RunArgs& ra,            \
+                             const OutBase& ob, unsigned long long* queue,   \
+                             int cap_ssa, int cap_leap, cudaStream_t st);
+PYST_DECL_SORTED(0)
+PYST_DECL_SORTED(1)
+#undef PYST_DECL_SORTED
+
 int launch_score_backward(const int32_t* samples, const double* score,
                           int64_t U, int kappa, int ita, int R,
                           const double* mean, const double* var,

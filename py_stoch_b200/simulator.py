@@ -78,12 +78,14 @@ def simulate(model, n_traj, method='direct', seed=0, traj_id_base=0,
              mapping='auto', device=None, stream=None, status=True,
              events=True, seqhash=False, t_final=False, score=False,
              step_budget=DEFAULT_STEP_BUDGET, ssa_fallback_steps=100, max_leap_retries=63,
-             block_size=0, out=None, d_blob=None):
+             block_size=0, out=None, d_blob=None, sorted_blocks=True):
     """Run ``n_traj`` trajectories of ``model`` (a :class:`Model`) on the GPU.
 
     Asynchronous on ``stream`` (default: torch's current stream).  ``out``
     may supply preallocated tensors by name; ``d_blob`` a device copy of
-    ``model.blob()``.
+    ``model.blob()``.  ``sorted_blocks=False`` selects the simple
+    one-trajectory-per-thread tau-leaping loop instead of the mode-sorted
+    block scheduler (identical results).
     """
     torch = _torch()
     device = torch.device(device or 'cuda')
@@ -120,7 +122,7 @@ def simulate(model, n_traj, method='direct', seed=0, traj_id_base=0,
     r = _lib.RunDesc(n, int(traj_id_base), int(seed) & 0xFFFFFFFFFFFFFFFF,
                      meth, _mapping(mapping), int(ssa_fallback_steps),
                      int(max_leap_retries), int(step_budget), int(block_size),
-                     0)
+                     0 if sorted_blocks else _lib.FLAG_UNSORTED)
     if stream is None:
         stream = torch.cuda.current_stream(device)
     sptr = C.c_void_p(stream.cuda_stream)

@@ -296,3 +296,21 @@ def test_batch_matches_single_runs(torch_cuda, built_lib, oracle_mod):
                                    o['t_final'], rtol=T_RTOL)
         np.testing.assert_allclose(b.score(i).cpu().numpy(), o['score'],
                                    rtol=T_RTOL, atol=1e-12)
+
+
+@pytest.mark.parametrize('score', [False, True])
+def test_sorted_scheduler_matches_unsorted(torch_cuda, built_lib, oracle_mod,
+                                           score):
+    """The mode-sorted block scheduler only reorders work: every output
+    equals the one-trajectory-per-thread loop and the oracle."""
+    m = networks.schlogl(t_end=2.0, n_samples=50)
+    n = 3000  # more trajectories than one block so slots are refilled
+    a = _gpu(torch_cuda, m, n, 'tau', 'thread', seed=8, score=score)
+    b = _gpu(torch_cuda, m, n, 'tau', 'thread', seed=8, score=score,
+             sorted_blocks=False)
+    for k in ('samples', 'status', 'events', 'seqhash', 't_final'):
+        np.testing.assert_array_equal(a[k], b[k])
+    if score:
+        np.testing.assert_array_equal(a['score'], b['score'])
+    _compare(a, _oracle(oracle_mod, m, n, 'tau', 'thread', seed=8),
+             score=score)
