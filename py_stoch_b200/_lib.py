@@ -10,7 +10,9 @@ import os
 import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, 'libpystoch_b200.so')
+# PYST_LIB selects another build of the library (e.g. an experimental one)
+LIB_PATH = os.environ.get('PYST_LIB') or os.path.join(_HERE,
+                                                       'libpystoch_b200.so')
 
 PYST_OK = 0
 PYST_EINVAL = 1

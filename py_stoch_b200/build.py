@@ -101,12 +101,16 @@ def up_to_date():
         return f.read().strip() == source_hash()
 
 
-def build(force=False, verbose=False, extra=(), jobs=None):
+def build(force=False, verbose=False, extra=(), jobs=None, lib=None,
+          build_dir=None):
     """Compile stale objects in parallel and relink; return the .so path.
 
     The library counts as current when its stamp file holds the content
     hash of the sources (modification times are not trusted: copies of the
     tree may not keep them)."""
+    if lib is not None:
+        # a variant build (other -D flags) into its own directory
+        return _build_variant(lib, build_dir, extra, verbose, jobs)
     if not force and not extra and up_to_date():
         return LIB
     os.makedirs(BUILD, exist_ok=True)
@@ -136,6 +140,23 @@ def build(force=False, verbose=False, extra=(), jobs=None):
     if extra and logs:
         print('\n'.join(l for l in logs if l.strip()))
     return LIB
+
+
+def _build_variant(lib, build_dir, extra, verbose, jobs):
+    os.makedirs(build_dir, exist_ok=True)
+    objs = []
+    todo = []
+    for src, obj, defs in units():
+        objp = os.path.join(build_dir, obj)
+        objs.append(objp)
+        todo.append((src, objp, defs))
+    jobs = jobs or max(1, min(len(todo), os.cpu_count() or 4))
+    with cf.ThreadPoolExecutor(jobs) as ex:
+        for fu in [ex.submit(_compile, s, o, d, extra, verbose)
+                   for s, o, d in todo]:
+            fu.result()
+    subprocess.check_call([nvcc()] + ARCH + ['-shared', '-o', lib] + objs)
+    return lib
 
 
 if __name__ == '__main__':

@@ -172,15 +172,17 @@ __device__ __forceinline__ void thread_init(const ModelView& m, int32_t* xcol,
 
 // Advance one trajectory.  Returns when it finishes, or -- for block
 // scheduling -- when it has taken cap_ssa SSA steps or cap_leap leaps in
-// this call, or when a DECIDE picks the other mode than the one the call
-// started in (stop_on_switch).  With unbounded caps this is the whole
+// this call, when the SM clock passes `deadline` (if non-zero), or when a
+// DECIDE picks the other mode than the one the call started in
+// (stop_on_switch).  It stops only between steps, so the trajectory resumes
+// exactly where it left off.  With unbounded caps this is the whole
 // trajectory.
 template <int MAXR, bool TAU, bool SCORE>
 __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
                              int bs, const RunArgs& ra, uint64_t traj_id,
                              TState& st, double* integ, int* cnt,
                              const TrajOut& o, int cap_ssa, int cap_leap,
-                             bool stop_on_switch) {
+                             bool stop_on_switch, long long deadline = 0) {
   const int S = m.S, R = m.R, ita = m.ita, kappa = m.kappa;
 #define XV(i) xcol[(int64_t)(i) * bs]
 #define SL(i) slot[(int64_t)(i) * bs]
@@ -204,6 +206,7 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
 
   while (true) {
     if (n_ssa >= cap_ssa || n_leap >= cap_leap) break;
+    if (deadline && (long long)clock64() > deadline) break;
     float a[MAXR];
     double a0 = 0.0;
 #pragma unroll

@@ -20,6 +20,17 @@ namespace PYST_CAT(sorted_flavour_, PYST_SCORE, ) {
 constexpr bool kScore = (bool)PYST_SCORE;
 constexpr int kBlock = kScore ? 128 : 256;
 
+// Blocks per SM the register allocation must allow (launch bounds).
+#ifndef PYST_SORTED_MINB
+#define PYST_SORTED_MINB 1
+#endif
+// Round length in SM clock cycles (0: rounds end only on the step caps).
+// A time box makes the warps of a block reach the regrouping barrier
+// together whatever mix of SSA steps and leaps they run.
+#ifndef PYST_ROUND_CYCLES
+#define PYST_ROUND_CYCLES 0
+#endif
+
 struct SortedSmem {
   uint32_t* blob;
   uint64_t* bar;
@@ -94,7 +105,7 @@ __device__ inline SortedSmem carve(unsigned char* p, int blob_words, int S,
 }
 
 template <int MAXR>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, PYST_SORTED_MINB)
     k_tau_sorted(const uint32_t* __restrict__ gblob, int blob_words,
                  int64_t n_traj, uint64_t id_base, RunArgs ra, OutBase ob,
                  unsigned long long* queue, int cap_ssa, int cap_leap) {
@@ -144,9 +155,11 @@ __global__ void __launch_bounds__(kBlock)
   while (true) {
     if (active) {
       const TrajOut o = ob.at(0, u, 0, 0, ob.stride, R);
+      const long long deadline =
+          PYST_ROUND_CYCLES ? (long long)clock64() + PYST_ROUND_CYCLES : 0;
       thread_round<MAXR, true, kScore>(m, xa + tid, slotc, kBlock, ra,
                                        id_base + (uint64_t)u, st, integ, cnt,
-                                       o, cap_ssa, cap_leap, true);
+                                       o, cap_ssa, cap_leap, true, deadline);
       if (st.flags & TS_DONE) {
         thread_finish<MAXR, kScore>(m, xa + tid, kBlock, st, integ, cnt, o);
         u = nthreads + (int64_t)atomicAdd(queue, 1ull);
