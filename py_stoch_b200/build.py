@@ -102,7 +102,7 @@ def up_to_date():
 
 
 def build(force=False, verbose=False, extra=(), jobs=None, lib=None,
-          build_dir=None):
+          build_dir=None, only=None):
     """Compile stale objects in parallel and relink; return the .so path.
 
     The library counts as current when its stamp file holds the content
@@ -110,7 +110,7 @@ def build(force=False, verbose=False, extra=(), jobs=None, lib=None,
     tree may not keep them)."""
     if lib is not None:
         # a variant build (other -D flags) into its own directory
-        return _build_variant(lib, build_dir, extra, verbose, jobs)
+        return _build_variant(lib, build_dir, extra, verbose, jobs, only)
     if not force and not extra and up_to_date():
         return LIB
     os.makedirs(BUILD, exist_ok=True)
@@ -142,11 +142,18 @@ def build(force=False, verbose=False, extra=(), jobs=None, lib=None,
     return LIB
 
 
-def _build_variant(lib, build_dir, extra, verbose, jobs):
+def _build_variant(lib, build_dir, extra, verbose, jobs, only=None):
+    """Link a library variant: units whose source is in `only` (default:
+    all) are recompiled with `extra` flags into build_dir, the rest are
+    taken from the default build."""
+    build()
     os.makedirs(build_dir, exist_ok=True)
     objs = []
     todo = []
     for src, obj, defs in units():
+        if only is not None and src not in only:
+            objs.append(os.path.join(BUILD, obj))
+            continue
         objp = os.path.join(build_dir, obj)
         objs.append(objp)
         todo.append((src, objp, defs))

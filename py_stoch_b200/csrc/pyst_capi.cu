@@ -32,8 +32,14 @@ namespace {
 
 // Round lengths of the mode-sorted tau-leaping kernel: SSA steps and leaps
 // a trajectory advances between two regroupings of its block.
-constexpr int kSortedCapSsa = 256;
-constexpr int kSortedCapLeap = 32;
+#ifndef PYST_CAP_SSA
+#define PYST_CAP_SSA 256
+#endif
+#ifndef PYST_CAP_LEAP
+#define PYST_CAP_LEAP 32
+#endif
+constexpr int kSortedCapSsa = PYST_CAP_SSA;
+constexpr int kSortedCapLeap = PYST_CAP_LEAP;
 
 int read_header(const uint32_t* h, HostModelInfo* mi) {
   if (!h) return PYST_EINVAL;
