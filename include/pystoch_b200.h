@@ -221,6 +221,28 @@ int pyst_score_backward(const int32_t* samples, const double* score,
                         void* d_workspace, size_t workspace_bytes,
                         void* stream);
 
+/* Same reduction as pyst_score_backward, for callers that cannot allocate
+ * the workspace themselves: a host runtime that has already handed all
+ * device memory to its own pool, or a loop that cannot accept the
+ * device-wide synchronisation a cudaMalloc may cause.  It allocates nothing
+ * (no cudaMalloc, cudaFree or allocating library call); its scratch is a
+ * fixed PYST_NOALLOC_SCRATCH_BYTES array inside the library that every GPU
+ * loading the library keeps until exit.  Calls needing more scratch than
+ * that -- ceil(n_traj / 256) * n_reactions * 8 bytes, i.e. n_traj up to
+ * 1,048,576 with 32 reactions -- return PYST_EUNSUPPORTED.  The first call
+ * on a device looks up the array's device address there (make that first
+ * call before any stream capture).  All calls share the one array, which
+ * keeps the last call's contents; calls that overlap on the GPU race, so
+ * serialise them (one stream, or events).  This entry point has no
+ * counterpart in the reference, which has no gradients. */
+#define PYST_NOALLOC_SCRATCH_BYTES (1 << 20)
+int pyst_score_backward_noalloc(const int32_t* samples, const double* score,
+                                int64_t n_traj, int32_t kappa, int32_t ita,
+                                int32_t n_reactions, const double* mean,
+                                const double* var, const double* gmean,
+                                const double* gvar, double* d_grad,
+                                void* stream);
+
 /* ---- misc -------------------------------------------------------------- */
 
 int pyst_abi_version(void);

@@ -41,6 +41,7 @@ MAX_REACTIONS = 4096
 THREAD_MAX_REACTIONS = 32
 MAX_BLOB_WORDS = 12288
 RUN_WORKSPACE_BYTES = 256
+NOALLOC_SCRATCH_BYTES = 1 << 20
 
 # header word indices (PYST_H_*)
 H_MAGIC, H_WORDS, H_S, H_R, H_KAPPA, H_ITA = 0, 1, 2, 3, 4, 5
@@ -111,6 +112,9 @@ SIGNATURES = {
     'pyst_score_backward': (C.c_int, [_p, _p, C.c_int64, C.c_int32,
                                       C.c_int32, C.c_int32, _p, _p, _p, _p,
                                       _p, _p, C.c_size_t, _p]),
+    'pyst_score_backward_noalloc': (C.c_int, [_p, _p, C.c_int64, C.c_int32,
+                                              C.c_int32, C.c_int32, _p, _p,
+                                              _p, _p, _p, _p]),
     'pyst_test_philox': (C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64,
                                    C.c_int64, _p, _p]),
     'pyst_test_philox_raw': (C.c_int, [_p, C.c_int64, _p, C.c_int, _p]),

@@ -1,6 +1,8 @@
 // Likelihood-ratio gradient reduction and the test hooks.
 #include <curand_kernel.h>
 
+#include <mutex>
+
 #include "pyst_launch.cuh"
 #include "pystoch_b200_testing.h"
 
@@ -124,11 +126,66 @@ int launch_score_backward(const int32_t* samples, const double* score,
   return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
 }
 
+// ---- allocation-free gradient reduction --------------------------------
+// Scratch of pyst_score_backward_noalloc: the per-block partial sums live in
+// this fixed array instead of caller workspace.  Every GPU that loads the
+// library holds PYST_NOALLOC_SCRATCH_BYTES of it until the process exits.
+static __device__ __align__(256) double
+    g_noalloc_scratch[PYST_NOALLOC_SCRATCH_BYTES / sizeof(double)];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device.  On the host
+// the symbol is only a stand-in; a kernel must be given this address.
+// Looked up once per device, the first time the entry point runs there.
+int noalloc_scratch(double** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return PYST_ECUDA;
+  if (dev < 0 || dev >= kMaxDevices) return PYST_EUNSUPPORTED;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p)
+      return PYST_ECUDA;
+    g_noalloc_ptr[dev] = (double*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return PYST_OK;
+}
+
+}  // namespace
+
 }  // namespace pyst
 
 using namespace pyst;
 
 extern "C" {
+
+int pyst_score_backward_noalloc(const int32_t* samples, const double* score,
+                                int64_t n_traj, int32_t kappa, int32_t ita,
+                                int32_t n_reactions, const double* mean,
+                                const double* var, const double* gmean,
+                                const double* gvar, double* d_grad,
+                                void* stream) {
+  if (!samples || !score || !mean || !gmean || !d_grad || n_traj < 1 ||
+      kappa < 1 || ita < 1 || n_reactions < 1)
+    return PYST_EINVAL;
+  if (gvar && !var) return PYST_EINVAL;
+  const int64_t nblk = score_backward_blocks(n_traj);
+  if ((uint64_t)nblk * (uint64_t)n_reactions * sizeof(double) >
+      (uint64_t)PYST_NOALLOC_SCRATCH_BYTES)
+    return PYST_EUNSUPPORTED;
+  double* part = nullptr;
+  const int rc = noalloc_scratch(&part);
+  if (rc) return rc;
+  return launch_score_backward(samples, score, n_traj, kappa, ita,
+                               n_reactions, mean, var, gmean, gvar, part,
+                               d_grad, (cudaStream_t)stream);
+}
 
 int pyst_test_philox(uint64_t seed, uint64_t id, uint64_t n0, int64_t count,
                      uint32_t* d_out, void* stream) {
