@@ -57,7 +57,7 @@ def test_autograd_matches_fp64_gradient(torch_cuda, telegraph_run):
     wv = rng.normal(size=var.shape) / 100.0
     loss = (mean * torch.from_numpy(wm).cuda()).sum() + (
         var * torch.from_numpy(wv).cuda()).sum()
-    (g,) = torch.autograd.grad(loss, logk)
+    (g,) = torch.autograd.grad(loss, logk, retain_graph=True)
     g = g.cpu().numpy()
     gm, gv = moments.moment_gradients(m)
     want = np.einsum('f,jf->j', wm[0], gm[:, 3]) + np.einsum(
@@ -80,7 +80,7 @@ def test_autograd_mean_matches_finite_differences(torch_cuda, telegraph_run):
     w = np.zeros(mean.shape)
     w[0, -1] = 1.0  # protein mean at t_end
     (g,) = torch.autograd.grad((mean * torch.from_numpy(w).cuda()).sum(),
-                               logk)
+                               logk, retain_graph=True)
     g = g.cpu().numpy()
     res = simulate(m, U, method='direct', seed=4, score=True)
     torch.cuda.synchronize()
