@@ -68,7 +68,9 @@ enum { PYST_FLAG_UNSORTED = 1 };
 /* Limits of this build. */
 #define PYST_MAX_SPECIES 1024
 #define PYST_MAX_REACTIONS 4096
-#define PYST_THREAD_MAX_REACTIONS 32  /* thread-per-trajectory kernels      */
+#define PYST_THREAD_MAX_REACTIONS 32  /* register-array thread kernels; above
+                                         it the thread mapping recomputes
+                                         propensities (no scores) */
 #define PYST_MAX_BLOB_WORDS 12288     /* model blob staged in 48 KiB smem   */
 
 /*

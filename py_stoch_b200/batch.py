@@ -38,11 +38,14 @@ def estimated_cost(model, method):
     return cost * (1.0 + model.n_reactions / 32.0)
 
 
-def auto_mapping(model):
-    if (model.n_reactions <= _lib.THREAD_MAX_REACTIONS
-            and model.n_species <= 64):
-        return _lib.MAP_THREAD
-    return _lib.MAP_WARP
+def auto_mapping(model, score=False):
+    """Thread per trajectory unless the species columns would not fit or
+    a scored model has more reactions than the register accumulators."""
+    if model.n_species > 64:
+        return _lib.MAP_WARP
+    if score and model.n_reactions > _lib.THREAD_MAX_REACTIONS:
+        return _lib.MAP_WARP
+    return _lib.MAP_THREAD
 
 
 class Batch(object):
@@ -73,8 +76,8 @@ class Batch(object):
         for m, x in zip(self.models, maps):
             x = _mapping(x)
             if x == _lib.MAP_AUTO:
-                x = auto_mapping(m)
-            if x == _lib.MAP_THREAD and (
+                x = auto_mapping(m, score)
+            if x == _lib.MAP_THREAD and score and (
                     m.n_reactions > _lib.THREAD_MAX_REACTIONS):
                 x = _lib.MAP_WARP
             mp.append(x)
@@ -150,9 +153,13 @@ class Batch(object):
 
     def run(self, seed=0, stream=None, ssa_fallback_steps=100,
             max_leap_retries=63, step_budget=None, block_size=0):
-        """Enqueue the whole batch on ``stream`` (one kernel launch)."""
+        """Enqueue the whole batch on ``stream`` (one kernel launch).
+        ``block_size`` 0 picks 64 threads when no item has more than 64
+        trajectories (one block then covers an item), else 128."""
         torch = _torch()
         L = _lib.lib()
+        if not block_size:
+            block_size = 64 if int(self.n_traj.max()) <= 64 else 128
         if step_budget is None:
             step_budget = DEFAULT_STEP_BUDGET
         o = self.out

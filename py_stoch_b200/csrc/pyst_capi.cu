@@ -121,10 +121,12 @@ int single_run(const uint32_t* h_blob, const uint32_t* d_blob,
   int mapping = run->mapping;
   const int bs = run->block_size ? run->block_size : 128;
   if (mapping == PYST_MAP_AUTO)
-    mapping = (mi.R <= PYST_THREAD_MAX_REACTIONS && mi.S <= 64)
+    mapping = (mi.S <= 64 && (mi.R <= PYST_THREAD_MAX_REACTIONS || !score))
                   ? PYST_MAP_THREAD
                   : PYST_MAP_WARP;
-  if (mapping == PYST_MAP_THREAD && mi.R > PYST_THREAD_MAX_REACTIONS)
+  // thread-mapped scores keep per-reaction accumulators in registers
+  if (mapping == PYST_MAP_THREAD && score &&
+      mi.R > PYST_THREAD_MAX_REACTIONS)
     return PYST_EUNSUPPORTED;
   const uint64_t idb = (uint64_t)run->traj_id_base;
   const int64_t n = run->n_traj;

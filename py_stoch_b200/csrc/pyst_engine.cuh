@@ -530,6 +530,312 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
 }
 
 // ===================================================================
+// one trajectory per thread, any number of reactions
+// ===================================================================
+// Same steps and arithmetic as thread_round, for R beyond the register
+// arrays: loops over reactions are not unrolled and propensities are
+// recomputed where thread_round reads a[j] again (selection pass, critical
+// sums, leap means), so nothing per reaction is stored.  The critical flag
+// of a reaction is re-derived from the species counts when needed.
+__device__ __forceinline__ bool is_critical(const ModelView& m, int j,
+                                            const int32_t* xcol, int bs) {
+  const int e1 = m.critptr(j + 1);
+  for (int e = m.critptr(j); e < e1; ++e) {
+    const uint32_t ce = m.crit(e);
+    if ((int64_t)(ce >> 16) * m.n_c >
+        (int64_t)xcol[(int64_t)ent_lo(ce) * bs])
+      return true;
+  }
+  return false;
+}
+
+template <bool TAU>
+__device__ void thread_round_big(const ModelView& m, int32_t* xcol,
+                                 int64_t* slot, int bs, const RunArgs& ra,
+                                 uint64_t traj_id, TState& st,
+                                 const TrajOut& o, int cap_ssa, int cap_leap,
+                                 bool stop_on_switch) {
+  const int S = m.S, R = m.R, ita = m.ita, kappa = m.kappa;
+#define XV(i) xcol[(int64_t)(i) * bs]
+#define SL(i) slot[(int64_t)(i) * bs]
+  Stream rs = make_stream(ra.seed, traj_id);
+  rs.n = st.n;
+  double t = st.t;
+  int f = st.f;
+  int64_t events = st.events, steps = st.steps;
+  uint64_t h = st.h;
+  int status = PYST_TRAJ_DONE;
+  bool fill_state = false, done = false;
+  const int64_t budget = ra.step_budget;
+  bool ssa_mode = (st.flags & TS_SSA) != 0;
+  const bool group_leap = (st.flags & TS_LEAPGRP) != 0;
+  bool leap_grp = group_leap;
+  int ssa_left = st.ssa_left;
+  uint32_t leap_q = st.leap_q;
+  int n_ssa = 0, n_leap = 0;
+  auto xget = [&](int i) { return XV(i); };
+
+  while (true) {
+    if (n_ssa >= cap_ssa || n_leap >= cap_leap) break;
+    double a0 = 0.0;
+    for (int j = 0; j < R; ++j)
+      a0 = __dadd_rn(a0, (double)propensity(m, j, xget));
+    if (a0 == 0.0) {
+      status = PYST_TRAJ_ABSORBED;
+      fill_state = true;
+      done = true;
+      break;
+    }
+    if (steps >= budget) {
+      status = PYST_TRAJ_STEP_BUDGET;
+      done = true;
+      break;
+    }
+    if (TAU && !ssa_mode) {
+      for (int i = 0; i < S; ++i) SL(i) = 0;
+      for (int j = 0; j < R; ++j) {
+        if (is_critical(m, j, xcol, bs)) continue;
+        const float aj = propensity(m, j, xget);
+        const int e1 = m.netptr(j + 1);
+        for (int e = m.netptr(j); e < e1; ++e) {
+          const uint32_t ne = m.net(e);
+          const int sp = ent_lo(ne);
+          const int v = ent_hi_s16(ne);
+          float2 ms = *reinterpret_cast<float2*>(&SL(sp));
+          ms.x = __fadd_rn(ms.x, __fmul_rn((float)v, aj));
+          ms.y = __fadd_rn(ms.y, __fmul_rn((float)(v * v), aj));
+          *reinterpret_cast<float2*>(&SL(sp)) = ms;
+        }
+      }
+      float tau1 = __int_as_float(0x7f800000);
+      for (int i = 0; i < S; ++i) {
+        const uint32_t gw = m.g(i);
+        if (!((gw >> 16) & 1u)) continue;
+        const float2 ms = *reinterpret_cast<float2*>(&SL(i));
+        const float c = tau_candidate(m.eta, gw, XV(i), ms.x, ms.y);
+        if (c < tau1) tau1 = c;
+      }
+      if ((double)tau1 < __ddiv_rn(10.0, a0)) {
+        ssa_mode = true;
+        ssa_left = ra.ssa_fallback_steps;
+        leap_grp = false;
+        if (stop_on_switch && group_leap) break;
+      } else {
+        leap_grp = true;
+        if (stop_on_switch && !group_leap) break;
+        steps++;
+        n_leap++;
+        double a0c = 0.0;
+        for (int j = 0; j < R; ++j)
+          if (is_critical(m, j, xcol, bs))
+            a0c = __dadd_rn(a0c, (double)propensity(m, j, xget));
+        double tau2 = __longlong_as_double(0x7ff0000000000000ll);
+        uint4 wc = make_uint4(0, 0, 0, 0);
+        if (a0c > 0.0) {
+          wc = next_block(rs);
+          tau2 = __ddiv_rn(-pyst_log(u53(wc.x, wc.y)), a0c);
+        }
+        const double tau1d = (double)tau1;
+        double tau = (tau2 < tau1d) ? tau2 : tau1d;
+        int kcrit = -1;
+        if (tau1d > tau2) {
+          const double r = __dmul_rn(u53(wc.z, wc.w), a0c);
+          double cum = 0.0;
+          int lastnz = -1;
+          for (int j = 0; j < R; ++j) {
+            if (!is_critical(m, j, xcol, bs)) continue;
+            const float aj = propensity(m, j, xget);
+            cum = __dadd_rn(cum, (double)aj);
+            if (aj > 0.0f) lastnz = j;
+            if (cum >= r) {
+              kcrit = j;
+              break;
+            }
+          }
+          if (kcrit < 0) kcrit = lastnz;
+        }
+        int retry = 0;
+        bool ok = false;
+        int64_t fired = 0;
+        uint64_t hl = 0;
+        while (true) {
+          // Poisson firings, accumulated straight into the state change
+          for (int i = 0; i < S; ++i) SL(i) = 0;
+          bool bad = false;
+          fired = 0;
+          hl = seq_mix(h, PYST_LEAP_TAG);
+          for (int j = 0; j < R; ++j) {
+            int kj;
+            if (is_critical(m, j, xcol, bs)) {
+              kj = (j == kcrit) ? 1 : 0;
+            } else {
+              const float lam =
+                  __fmul_rn(propensity(m, j, xget), (float)tau);
+              const int k = poisson(lam, leap_key(rs, leap_q, j, retry));
+              if (k < 0) bad = true;
+              kj = k < 0 ? 0 : k;
+            }
+            if (kj != 0) {
+              fired += kj;
+              hl = seq_mix(hl, ((uint64_t)j << 32) | (uint32_t)kj);
+              const int e1 = m.netptr(j + 1);
+              for (int e = m.netptr(j); e < e1; ++e) {
+                const uint32_t ne = m.net(e);
+                SL(ent_lo(ne)) += (int64_t)kj * ent_hi_s16(ne);
+              }
+            }
+          }
+          if (bad) {
+            status = PYST_TRAJ_SAMPLER;
+            break;
+          }
+          bool neg = false, over = false;
+          for (int i = 0; i < S; ++i) {
+            const int64_t nx = (int64_t)XV(i) + SL(i);
+            neg |= nx < 0;
+            over |= nx > PYST_I32MAX;
+          }
+          if (over) {
+            status = PYST_TRAJ_OVERFLOW;
+            break;
+          }
+          if (!neg) {
+            ok = true;
+            break;
+          }
+          tau = __dmul_rn(tau, 0.5);
+          retry++;
+          if (retry > ra.max_leap_retries) {
+            status = PYST_TRAJ_LEAP_RETRY;
+            break;
+          }
+        }
+        if (!ok) {
+          done = true;
+          break;
+        }
+        leap_q++;
+        h = hl;
+        const double tn = __dadd_rn(t, tau);
+        while (tn >= m.time(f)) {
+          const double frac = __ddiv_rn(__dsub_rn(m.time(f), t), tau);
+          for (int k = 0; k < kappa; ++k) {
+            const int i = m.out(k);
+            const double inc = rint(__dmul_rn((double)SL(i), frac));
+            store_sample(o, ita, k, f, XV(i) + (int)inc);
+          }
+          f++;
+          if (f == ita) {
+            done = true;
+            break;
+          }
+        }
+        for (int i = 0; i < S; ++i) XV(i) = (int)((int64_t)XV(i) + SL(i));
+        events += fired;
+        t = tn;
+        if (done) break;
+        continue;
+      }
+    }
+    // ------------------------ one direct-method step -------------------
+    steps++;
+    n_ssa++;
+    const uint4 w = next_block(rs);
+    const double tau = __ddiv_rn(-pyst_log(u53(w.x, w.y)), a0);
+    const double r = __dmul_rn(u53(w.z, w.w), a0);
+    int sel = -1;
+    {
+      double cum = 0.0;
+      int lastnz = -1;
+      for (int j = 0; j < R; ++j) {
+        const float aj = propensity(m, j, xget);
+        cum = __dadd_rn(cum, (double)aj);
+        if (aj > 0.0f) lastnz = j;
+        if (cum >= r) {
+          sel = j;
+          break;
+        }
+      }
+      if (sel < 0) sel = lastnz;
+    }
+    const double tn = __dadd_rn(t, tau);
+    while (tn >= m.time(f)) {
+      for (int k = 0; k < kappa; ++k) store_sample(o, ita, k, f, XV(m.out(k)));
+      f++;
+      if (f == ita) {
+        done = true;
+        break;
+      }
+    }
+    t = tn;
+    if (done) break;
+    {
+      const int e1 = m.netptr(sel + 1);
+      bool over = false;
+      for (int e = m.netptr(sel); e < e1; ++e) {
+        const uint32_t ne = m.net(e);
+        const int sp = ent_lo(ne);
+        const int64_t nx = (int64_t)XV(sp) + ent_hi_s16(ne);
+        if (nx < 0 || nx > PYST_I32MAX) over = true;
+        else XV(sp) = (int)nx;
+      }
+      if (over) {
+        status = PYST_TRAJ_OVERFLOW;
+        done = true;
+        break;
+      }
+    }
+    events++;
+    h = seq_mix(h, (uint64_t)sel);
+    if (TAU) {
+      if (--ssa_left <= 0) ssa_mode = false;
+    }
+  }
+  st.t = t;
+  st.n = rs.n;
+  st.events = events;
+  st.steps = steps;
+  st.h = h;
+  st.f = f;
+  st.leap_q = leap_q;
+  st.ssa_left = ssa_left;
+  st.flags = (ssa_mode ? TS_SSA : 0) | (leap_grp ? TS_LEAPGRP : 0) |
+             (done ? TS_DONE : 0) | (fill_state ? TS_FILL : 0) |
+             (status << 8);
+#undef XV
+#undef SL
+}
+
+// thread_round for MAXR > 0 (register arrays), thread_round_big for 0
+template <int MAXR, bool TAU, bool SCORE>
+__device__ __forceinline__ void any_round(
+    const ModelView& m, int32_t* xcol, int64_t* slot, int bs,
+    const RunArgs& ra, uint64_t traj_id, TState& st, double* integ, int* cnt,
+    const TrajOut& o, int cap_ssa, int cap_leap, bool stop_on_switch,
+    long long deadline) {
+  if constexpr (MAXR == 0) {
+    static_assert(!SCORE, "the large-R thread engine keeps no scores");
+    thread_round_big<TAU>(m, xcol, slot, bs, ra, traj_id, st, o, cap_ssa,
+                          cap_leap, stop_on_switch);
+  } else {
+    thread_round<MAXR, TAU, SCORE>(m, xcol, slot, bs, ra, traj_id, st, integ,
+                                   cnt, o, cap_ssa, cap_leap, stop_on_switch,
+                                   deadline);
+  }
+}
+
+template <bool TAU>
+__device__ void run_thread_big(const ModelView& m, int32_t* xcol,
+                               int64_t* slot, int bs, const RunArgs& ra,
+                               uint64_t traj_id, const TrajOut& o) {
+  TState st;
+  thread_init<TAU>(m, xcol, bs, st);
+  thread_round_big<TAU>(m, xcol, slot, bs, ra, traj_id, st, o, 0x7fffffff,
+                        0x7fffffff, false);
+  thread_finish<1, false>(m, xcol, bs, st, nullptr, nullptr, o);
+}
+
+// ===================================================================
 // one trajectory per warp
 // ===================================================================
 // Per-warp shared memory: x[S] int32, a[R] float, slot[S] 8 bytes,

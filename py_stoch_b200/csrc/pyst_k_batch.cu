@@ -62,9 +62,13 @@ __global__ void __launch_bounds__(128)
         if (m.R <= 8) {
           if (tau) run_thread<8, true, SCORE>(m, xcol, slot, bs, ra, id, o);
           else run_thread<8, false, SCORE>(m, xcol, slot, bs, ra, id, o);
-        } else {
+        } else if (SCORE || m.R <= PYST_THREAD_MAX_REACTIONS) {
+          // (the host maps scored items with more reactions to warps)
           if (tau) run_thread<32, true, SCORE>(m, xcol, slot, bs, ra, id, o);
           else run_thread<32, false, SCORE>(m, xcol, slot, bs, ra, id, o);
+        } else {
+          if (tau) run_thread_big<true>(m, xcol, slot, bs, ra, id, o);
+          else run_thread_big<false>(m, xcol, slot, bs, ra, id, o);
         }
       }
     } else {

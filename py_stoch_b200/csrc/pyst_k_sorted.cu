@@ -139,11 +139,12 @@ __global__ void __launch_bounds__(kBlock, PYST_SORTED_MINB)
   int32_t* xb = sm.xb;
   int64_t* slotc = sm.slot + tid;
   TState st;
-  double integ[kScore ? MAXR : 1];
-  int cnt[kScore ? MAXR : 1];
+  constexpr int kAcc = (kScore && MAXR > 0) ? MAXR : 1;
+  double integ[kAcc];
+  int cnt[kAcc];
   auto zero_score = [&]() {
 #pragma unroll
-    for (int j = 0; j < (kScore ? MAXR : 1); ++j) {
+    for (int j = 0; j < kAcc; ++j) {
       integ[j] = 0.0;
       cnt[j] = 0;
     }
@@ -159,11 +160,12 @@ __global__ void __launch_bounds__(kBlock, PYST_SORTED_MINB)
       const TrajOut o = ob.at(0, u, 0, 0, ob.stride, R);
       const long long deadline =
           PYST_ROUND_CYCLES ? (long long)clock64() + PYST_ROUND_CYCLES : 0;
-      thread_round<MAXR, true, kScore>(m, xa + tid, slotc, kBlock, ra,
-                                       id_base + (uint64_t)u, st, integ, cnt,
-                                       o, cap_ssa, cap_leap, true, deadline);
+      any_round<MAXR, true, kScore>(m, xa + tid, slotc, kBlock, ra,
+                                    id_base + (uint64_t)u, st, integ, cnt, o,
+                                    cap_ssa, cap_leap, true, deadline);
       if (st.flags & TS_DONE) {
-        thread_finish<MAXR, kScore>(m, xa + tid, kBlock, st, integ, cnt, o);
+        thread_finish<(MAXR > 0 ? MAXR : 1), kScore>(m, xa + tid, kBlock, st,
+                                                     integ, cnt, o);
         u = nthreads + (int64_t)atomicAdd(queue, 1ull);
         active = u < n_traj;
         zero_score();
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(kBlock, PYST_SORTED_MINB)
       xb[(int64_t)i * kBlock + rank] = xa[(int64_t)i * kBlock + tid];
     if (kScore) {
 #pragma unroll
-      for (int j = 0; j < (kScore ? MAXR : 1); ++j) {
+      for (int j = 0; j < kAcc; ++j) {
         sm.integ[j * kBlock + rank] = integ[j];
         sm.cnt[j * kBlock + rank] = cnt[j];
       }
@@ -229,7 +231,7 @@ __global__ void __launch_bounds__(kBlock, PYST_SORTED_MINB)
     st.flags = sm.flags[tid];
     if (kScore) {
 #pragma unroll
-      for (int j = 0; j < (kScore ? MAXR : 1); ++j) {
+      for (int j = 0; j < kAcc; ++j) {
         integ[j] = sm.integ[j * kBlock + tid];
         cnt[j] = sm.cnt[j * kBlock + tid];
       }
@@ -246,7 +248,7 @@ int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
                uint64_t id_base, const RunArgs& ra, const OutBase& ob,
                unsigned long long* queue, cudaStream_t st, int cap_ssa,
                int cap_leap) {
-  const size_t smem = sorted_smem_bytes(mi.words, mi.S, MR);
+  const size_t smem = sorted_smem_bytes(mi.words, mi.S, MR > 0 ? MR : 1);
   if (smem > kMaxDynSmem) return PYST_EUNSUPPORTED;
   auto kf = k_tau_sorted<MR>;
   const int rc = set_smem(kf, smem);
@@ -273,6 +275,13 @@ int PYST_CAT(launch_tau_sorted_, PYST_SCORE, )(
   if (cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st) !=
       cudaSuccess)
     return PYST_ECUDA;
+#if !PYST_SCORE
+  if (maxr > PYST_THREAD_MAX_REACTIONS)
+    return launch_one<0>(d_blob, mi, n, id_base, ra, ob, queue, st, cap_ssa,
+                         cap_leap);
+#else
+  if (maxr > PYST_THREAD_MAX_REACTIONS) return PYST_EUNSUPPORTED;
+#endif
   if (maxr <= 4)
     return launch_one<4>(d_blob, mi, n, id_base, ra, ob, queue, st, cap_ssa,
                          cap_leap);

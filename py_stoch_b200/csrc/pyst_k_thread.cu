@@ -52,8 +52,11 @@ __global__ void __launch_bounds__(128)
   int64_t* slot = (int64_t*)(xbase + (size_t)m.S * bs) + threadIdx.x;
   while (u < n_traj) {
     const TrajOut o = ob.at(0, u, 0, 0, ob.stride, m.R);
-    run_thread<MAXR, TAU, SCORE>(m, xcol, slot, bs, ra,
-                                 id_base + (uint64_t)u, o);
+    if constexpr (MAXR == 0)
+      run_thread_big<TAU>(m, xcol, slot, bs, ra, id_base + (uint64_t)u, o);
+    else
+      run_thread<MAXR, TAU, SCORE>(m, xcol, slot, bs, ra,
+                                   id_base + (uint64_t)u, o);
     u = nthreads + (int64_t)atomicAdd(queue, 1ull);
   }
 }
@@ -90,6 +93,12 @@ int PYST_CAT(launch_plain_thread_, PYST_TAU, PYST_SCORE)(
   if (cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st) !=
       cudaSuccess)
     return PYST_ECUDA;
+#if !PYST_SCORE
+  if (maxr > PYST_THREAD_MAX_REACTIONS)
+    return launch_one<0>(d_blob, mi, n, id_base, ra, ob, bs, st, smem, queue);
+#else
+  if (maxr > PYST_THREAD_MAX_REACTIONS) return PYST_EUNSUPPORTED;
+#endif
   if (maxr <= 4)
     return launch_one<4>(d_blob, mi, n, id_base, ra, ob, bs, st, smem, queue);
   if (maxr <= 8)

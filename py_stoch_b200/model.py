@@ -178,10 +178,11 @@ class Model(object):
         S, R = pre.shape
         k = np.asarray(k, dtype=np.float64).reshape(R)
         if combinatorial:
-            div = np.array([np.prod([math.factorial(int(n))
-                                     for n in pre[:, j]]) for j in range(R)],
-                           dtype=np.float64)
-            k = k / div
+            if pre.max(initial=0) > 20:
+                raise ValueError('stoichiometry above 20')
+            fact = np.array([math.factorial(n) for n in range(21)],
+                            dtype=np.float64)
+            k = k / fact[pre].prod(axis=0)
         if out_species is None:
             out_species = np.arange(S)
         return cls(pre, pre, post - pre, k, x0, sample_times, out_species,
@@ -250,13 +251,8 @@ def derive_hors(pre, order):
     that mentions exactly its reactants."""
     pre = np.asarray(pre)
     order = np.asarray(order)
-    S, R = pre.shape
     tot = order.sum(axis=0)
-    hor = np.zeros(S, np.int32)
-    hty = np.zeros(S, np.int32)
-    for i in range(S):
-        for j in range(R):
-            if order[i, j] > 0:
-                hor[i] = max(hor[i], tot[j])
-                hty[i] = max(hty[i], pre[i, j])
-    return hor, hty
+    mask = order > 0
+    hor = np.where(mask, tot[None, :], 0).max(axis=1, initial=0)
+    hty = np.where(mask, pre, 0).max(axis=1, initial=0)
+    return hor.astype(np.int32), hty.astype(np.int32)

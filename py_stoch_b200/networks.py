@@ -79,24 +79,35 @@ def telegraph(k=TELEGRAPH_NOMINAL, t_end=50.0, n_samples=20,
 def synthetic_networks(n_networks, seed=0, s_range=(5, 64), r_range=(8, 256),
                        n_samples=50, k_range=(1e-3, 1e1), x0_max=1000,
                        t_range=(1.0, 100.0)):
-    """Seeded uneven mass-action networks (list of :class:`Model`)."""
+    """Seeded uneven mass-action networks (list of :class:`Model`).
+
+    Per network: S ~ U{s_range}, R ~ U{r_range}; each reaction draws 0-2
+    distinct reactant species and 0-2 distinct product species, each with
+    stoichiometry 1 or 2; rate constants log-uniform in k_range (stochastic
+    mass action k * prod C(x_i, n_i)); x0 ~ U{0..x0_max}; t_end log-uniform
+    in t_range; all species recorded at n_samples times."""
     rng = np.random.default_rng(seed)
+    lk0, lk1 = np.log(k_range[0]), np.log(k_range[1])
+    lt0, lt1 = np.log(t_range[0]), np.log(t_range[1])
     out = []
     for _ in range(n_networks):
         S = int(rng.integers(s_range[0], s_range[1] + 1))
         R = int(rng.integers(r_range[0], r_range[1] + 1))
-        pre = np.zeros((S, R), np.int64)
-        post = np.zeros((S, R), np.int64)
-        for j in range(R):
-            for mat in (pre, post):
-                n = int(rng.integers(0, 3))
-                sp = rng.choice(S, size=n, replace=False)
-                for i in sp:
-                    mat[i, j] = int(rng.integers(1, 3))
-        k = np.exp(rng.uniform(np.log(k_range[0]), np.log(k_range[1]), R))
+        mats = []
+        for _side in range(2):
+            n = rng.integers(0, 3, R)                      # species per side
+            order = np.argsort(rng.random((R, S)), axis=1)[:, :2]
+            st = rng.integers(1, 3, (R, 2))
+            mat = np.zeros((S, R), np.int64)
+            cols = np.arange(R)
+            for q in range(2):
+                use = n > q
+                mat[order[use, q], cols[use]] = st[use, q]
+            mats.append(mat)
+        pre, post = mats
+        k = np.exp(rng.uniform(lk0, lk1, R))
         x0 = rng.integers(0, x0_max + 1, S)
-        t_end = float(np.exp(rng.uniform(np.log(t_range[0]),
-                                         np.log(t_range[1]))))
+        t_end = float(np.exp(rng.uniform(lt0, lt1)))
         m = Model.mass_action(pre, post, k, x0, _times(t_end, n_samples),
                               np.arange(S), t_max=t_end)
         m.name = 'synthetic'

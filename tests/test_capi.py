@@ -87,13 +87,15 @@ def test_run_rejects_bad_arguments(built_lib):
     r.block_size = 100
     assert L.pyst_tau_leap_run(blob.ctypes.data, 16, C.byref(r), C.byref(o),
                                8, 256, None) == _lib.PYST_EINVAL
-    # thread mapping on a model with too many reactions
+    # thread mapping with scores on a model with too many reactions
     big = networks.synthetic_networks(1, seed=1, r_range=(100, 100))[0]
     r.block_size = 0
     r.mapping = _lib.MAP_THREAD
+    o.score = 4096
     assert L.pyst_tau_leap_run(big.blob().ctypes.data, 16, C.byref(r),
                                C.byref(o), 8, 256,
                                None) == _lib.PYST_EUNSUPPORTED
+    o.score = 0
     ws = C.c_size_t(0)
     assert L.pyst_run_workspace_size(C.byref(r), C.byref(ws)) == 0
     assert ws.value == _lib.RUN_WORKSPACE_BYTES
