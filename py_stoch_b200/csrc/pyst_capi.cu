@@ -131,11 +131,16 @@ int single_run(const uint32_t* h_blob, const uint32_t* d_blob,
   const uint64_t idb = (uint64_t)run->traj_id_base;
   const int64_t n = run->n_traj;
   if (mapping == PYST_MAP_THREAD && tau &&
-      !(run->flags & PYST_FLAG_UNSORTED))
-    return score ? launch_tau_sorted_1(mi.R, d_blob, mi, n, idb, ra, ob, queue,
-                                       kSortedCapSsa, kSortedCapLeap, st)
-                 : launch_tau_sorted_0(mi.R, d_blob, mi, n, idb, ra, ob, queue,
-                                       kSortedCapSsa, kSortedCapLeap, st);
+      !(run->flags & PYST_FLAG_UNSORTED)) {
+    const int rc =
+        score ? launch_tau_sorted_1(mi.R, d_blob, mi, n, idb, ra, ob, queue,
+                                    kSortedCapSsa, kSortedCapLeap, st)
+              : launch_tau_sorted_0(mi.R, d_blob, mi, n, idb, ra, ob, queue,
+                                    kSortedCapSsa, kSortedCapLeap, st);
+    // the sorted block keeps every slot's species in shared memory; for
+    // models with too many species fall back to the unsorted loop
+    if (rc != PYST_EUNSUPPORTED) return rc;
+  }
   if (mapping == PYST_MAP_THREAD) {
     if (tau)
       return score ? launch_plain_thread_11(mi.R, d_blob, mi, n, idb, ra, ob,

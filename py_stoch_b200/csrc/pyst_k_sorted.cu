@@ -253,6 +253,9 @@ int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
   auto kf = k_tau_sorted<MR>;
   const int rc = set_smem(kf, smem);
   if (rc) return rc;
+  if (cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st) !=
+      cudaSuccess)
+    return PYST_ECUDA;
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf, kBlock, smem);
   if (per_sm < 1) per_sm = 1;
@@ -272,9 +275,6 @@ int PYST_CAT(launch_tau_sorted_, PYST_SCORE, )(
     uint64_t id_base, const RunArgs& ra, const OutBase& ob,
     unsigned long long* queue, int cap_ssa, int cap_leap, cudaStream_t st) {
   if (n <= 0) return PYST_OK;
-  if (cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st) !=
-      cudaSuccess)
-    return PYST_ECUDA;
 #if !PYST_SCORE
   if (maxr > PYST_THREAD_MAX_REACTIONS)
     return launch_one<0>(d_blob, mi, n, id_base, ra, ob, queue, st, cap_ssa,
