@@ -179,6 +179,113 @@ def run_reference(args, wl):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# batched persistent form vs plain one-launch-per-model form
+# ---------------------------------------------------------------------------
+def _events_timed(fn, stream):
+    import torch
+    torch.cuda.synchronize()
+    st = torch.cuda.Event(enable_timing=True)
+    en = torch.cuda.Event(enable_timing=True)
+    st.record(stream)
+    out = fn()
+    en.record(stream)
+    en.synchronize()
+    return st.elapsed_time(en), out
+
+
+def batch_vs_plain(kind, dev, subset=256, steps=1, full=True, budget=20000):
+    """Events/s of the batched form (one persistent launch, CUDA graph) and
+    of the plain form (one launch per model) on the same models.
+
+    kind 'sweep': Lotka-Volterra / Schlogl parameter sets within a decade of
+    the nominals, 256 trajectories each, tau-leaping with SSA fallback,
+    likelihood-ratio scores plus in-kernel statistics and Jacobians
+    (batched+grad).  kind 'synthetic': 4096 uneven synthetic networks, 64
+    trajectories each, tau-leaping.  Both forms run the same trajectories
+    with the same step budget and produce identical per-trajectory results;
+    only the scheduling differs."""
+    import torch
+    from py_stoch_b200 import networks
+    from py_stoch_b200.autotune import Autotuner
+    from py_stoch_b200.batch import Batch
+    from py_stoch_b200.simulator import simulate
+    stream = torch.cuda.current_stream(dev)
+    if kind == 'sweep':
+        models, _ = networks.parameter_sweep(16384, seed=1)
+        n_traj, grad = 256, True
+        desc = ('16384 parameter sets (Lotka-Volterra / Schlogl nominals '
+                '+-1 decade) x 256 trajectories, 50 samples, tau-leaping '
+                'with SSA fallback, scores + in-kernel mean/var/lag-1 + '
+                'Jacobians')
+    else:
+        models = networks.synthetic_networks(4096, seed=0)
+        n_traj, grad = 64, False
+        desc = ('4096 synthetic networks (S 5-64, R 8-256) x 64 '
+                'trajectories, 50 samples, tau-leaping with SSA fallback')
+    tuner = Autotuner(device=dev, score=grad)
+    tuner.tune(models, 'tau')
+    rng = np.random.default_rng(7)
+    pick = sorted(rng.permutation(len(models))[:subset].tolist())
+    sub = [models[i] for i in pick]
+    res = {'workload': desc, 'step_budget': budget,
+           'subset_models': len(sub)}
+
+    def batched(ms, ids=None):
+        b = Batch(ms, n_traj, method='tau', mapping_fn=tuner.mapping_fn,
+                  device=dev, score=grad, stats=grad, jacobian=grad,
+                  traj_id_base=ids)
+        g = b.graph(seed=11, step_budget=budget)
+        g.replay()
+        tot_ms, ev = 0.0, 0.0
+        for _ in range(steps):
+            ms_, _ = _events_timed(g.replay, stream)
+            tot_ms += ms_
+            ev += float(b.out['events'].sum().item())
+        st = torch.bincount(b.out['status'].long(), minlength=7).tolist()
+        del g
+        return tot_ms / steps, ev / steps, st, b
+
+    ids = [i * n_traj for i in pick]
+    ms_b, ev_b, st_b, _ = batched(sub, ids)
+    # plain form: one simulate() launch per model, same ids and budget
+    outs = [{'samples': torch.empty((m.kappa, m.ita, n_traj),
+                                    dtype=torch.int32, device=dev),
+             'events': torch.empty(n_traj, dtype=torch.int64, device=dev)}
+            for m in sub]
+
+    def plain():
+        for k, (m, i) in enumerate(zip(sub, pick)):
+            simulate(m, n_traj, method='tau', seed=11,
+                     traj_id_base=i * n_traj, device=dev, stream=stream,
+                     out=outs[k], score=grad, status=False,
+                     step_budget=budget,
+                     mapping=('thread' if tuner.mapping(m, 'tau') == 1
+                              else 'warp'))
+    plain()
+    ms_p, _ = _events_timed(plain, stream)
+    ev_p = float(sum(int(o['events'].sum().item()) for o in outs))
+    res['plain'] = {'ms': ms_p, 'events': ev_p, 'events_per_s':
+                    ev_p / ms_p * 1e3, 'launches': len(sub)}
+    res['batched_same_models'] = {'ms': ms_b, 'events': ev_b,
+                                  'events_per_s': ev_b / ms_b * 1e3,
+                                  'launches': 1, 'status_counts': st_b}
+    res['batched_over_plain'] = (ev_b / ms_b) / (ev_p / ms_p)
+    if full:
+        ms_f, ev_f, st_f, b = batched(models)
+        res['batched_full'] = {'models': len(models), 'ms': ms_f,
+                               'events': ev_f,
+                               'events_per_s': ev_f / ms_f * 1e3,
+                               'trajectories_per_s':
+                                   len(models) * n_traj / ms_f * 1e3,
+                               'status_counts': st_f}
+        del b
+    res['autotune'] = {k: v['mapping'] for k, v in tuner.table.items()
+                       if 'mapping' in v}
+    torch.cuda.empty_cache()
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -189,7 +296,11 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--n-traj', type=int, default=0,
                     help='override trajectories per GPU (profiling runs)')
+    ap.add_argument('--no-forms', action='store_true',
+                    help='skip the batched-vs-plain comparison')
     args = ap.parse_args()
+    if args.workload in ('sweep', 'synthetic'):
+        return forms_main(args)
     wl = workloads()[args.workload]
     if args.n_traj:
         wl['n'] = args.n_traj
@@ -322,9 +433,32 @@ def main():
         }
         if not args.no_cpu_baseline and world == 1:
             line['cpu_baseline'] = cpu_baseline(wl)
+        if not args.no_forms and world == 1:
+            line['forms'] = batch_vs_plain('sweep', dev, full=False)
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+    return 0
+
+
+def forms_main(args):
+    """--workload sweep | synthetic: the batched-vs-plain comparison as the
+    JSON line (value = batched events/s over all models)."""
+    import torch
+    from py_stoch_b200 import build as _build
+    dev = torch.device('cuda', int(os.environ.get('LOCAL_RANK', '0')))
+    torch.cuda.set_device(dev)
+    _build.build()
+    r = batch_vs_plain(args.workload, dev, steps=args.steps, full=True)
+    full = r['batched_full']
+    line = {'metric': METRIC, 'value': full['events_per_s'], 'unit': UNIT,
+            'n_gpus': 1, 'steps': args.steps, 'warmup': 1,
+            'ms_per_step': full['ms'], 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32/f64',
+            'data': 'synthetic', 'config': {'workload': r['workload']},
+            'trajectories_per_s': full['trajectories_per_s'],
+            'forms': r, 'gpu_launches': args.steps}
+    print(json.dumps(line))
     return 0
 
 

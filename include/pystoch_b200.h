@@ -127,6 +127,10 @@ typedef struct pyst_outputs {
   uint64_t* seqhash;  /* [n_traj] FNV-1a hash of the firing sequence        */
   double* t_final;    /* [n_traj] clock when the trajectory stopped         */
   double* score;      /* [n_traj][R] d log p / d log rate_j                 */
+  double* stats;      /* batched runs: per item [kappa][ita][3] mean,
+                         variance, lag-1 correlation with the next sample */
+  double* jacobian;   /* batched runs with scores: per item [2][kappa][ita][R]
+                         d mean / d log rate_j, d variance / d log rate_j  */
 } pyst_outputs;
 
 /* ---- model blob (host side, no CUDA) ----------------------------------- */
@@ -180,6 +184,8 @@ typedef struct pyst_batch_item {
   int64_t sample_offset;   /* element offset of its [kappa][ita][n_traj]   */
   int64_t traj_offset;     /* element offset into status/events/... arrays */
   int64_t score_offset;    /* element offset into score ([n_traj][R])      */
+  int64_t stats_offset;    /* element offset into stats                    */
+  int64_t jac_offset;      /* element offset into jacobian                 */
   int32_t method;          /* PYST_METHOD_*                                */
   int32_t mapping;         /* PYST_MAP_THREAD or PYST_MAP_WARP             */
 } pyst_batch_item;
@@ -199,7 +205,13 @@ int pyst_batch_workspace_size(int64_t n_items, size_t* bytes);
  * holding n_items pyst_batch_item; blocks take items from a device work
  * queue in array order (put expensive items first).  Per-trajectory output
  * pointers in `out` are bases that the item offsets index.  The run fields
- * n_traj, traj_id_base, method and mapping are taken from the items. */
+ * n_traj, traj_id_base, method and mapping are taken from the items.
+ * When `out->stats` / `out->jacobian` are set, the block that ran an item
+ * reduces its samples (and scores) into the item's summary statistics and
+ * their likelihood-ratio Jacobians in the same launch, in a fixed order.
+ * Variances are population variances; the lag-1 entry of sample f is the
+ * correlation of samples f and f+1 across trajectories (0 for the last
+ * sample or a zero variance). */
 int pyst_batch_run(const uint32_t* d_blobs, const pyst_batch_item* d_items,
                    int64_t n_items, const pyst_batch_limits* limits,
                    const pyst_run_desc* run, const pyst_outputs* out,

@@ -71,13 +71,14 @@ class RunDesc(C.Structure):
 class Outputs(C.Structure):
     _fields_ = [('samples', _p), ('out_stride', C.c_int64), ('status', _p),
                 ('events', _p), ('seqhash', _p), ('t_final', _p),
-                ('score', _p)]
+                ('score', _p), ('stats', _p), ('jacobian', _p)]
 
 
 class BatchItem(C.Structure):
     _fields_ = [('blob_offset', C.c_int64), ('n_traj', C.c_int64),
                 ('traj_id_base', C.c_int64), ('sample_offset', C.c_int64),
                 ('traj_offset', C.c_int64), ('score_offset', C.c_int64),
+                ('stats_offset', C.c_int64), ('jac_offset', C.c_int64),
                 ('method', C.c_int32), ('mapping', C.c_int32)]
 
 

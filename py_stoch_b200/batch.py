@@ -54,7 +54,7 @@ class Batch(object):
     def __init__(self, models, n_traj, method='direct', mapping='auto',
                  traj_id_base=None, device=None, score=False, status=True,
                  events=True, seqhash=False, t_final=False, order='cost',
-                 mapping_fn=None):
+                 mapping_fn=None, stats=False, jacobian=False):
         torch = _torch()
         self.device = torch.device(device or 'cuda')
         self.models = list(models)
@@ -99,6 +99,13 @@ class Batch(object):
             [[0], np.cumsum(self.n_traj)[:-1]]).astype(np.int64)
         self.score_offset = np.concatenate(
             [[0], np.cumsum(self.n_traj * self.R)[:-1]]).astype(np.int64)
+        self.stats_offset = np.concatenate(
+            [[0], np.cumsum(self.kappa * self.ita * 3)[:-1]]).astype(np.int64)
+        self.jac_offset = np.concatenate(
+            [[0], np.cumsum(2 * self.kappa * self.ita * self.R)[:-1]]
+        ).astype(np.int64)
+        if jacobian and not score:
+            raise ValueError('jacobian needs score=True')
         self.total_traj = int(self.n_traj.sum())
 
         if order == 'cost':
@@ -116,6 +123,8 @@ class Batch(object):
             it.sample_offset = int(self.sample_offset[i])
             it.traj_offset = int(self.traj_offset[i])
             it.score_offset = int(self.score_offset[i])
+            it.stats_offset = int(self.stats_offset[i])
+            it.jac_offset = int(self.jac_offset[i])
             it.method = int(self.methods[i])
             it.mapping = int(self.mappings[i])
         raw = np.frombuffer(bytes(items), dtype=np.uint8)
@@ -150,6 +159,14 @@ class Batch(object):
         if score:
             self.out['score'] = torch.empty(int((self.n_traj * self.R).sum()),
                                             dtype=torch.float64, device=dev)
+        if stats:
+            self.out['stats'] = torch.empty(
+                int((self.kappa * self.ita * 3).sum()), dtype=torch.float64,
+                device=dev)
+        if jacobian:
+            self.out['jacobian'] = torch.empty(
+                int((2 * self.kappa * self.ita * self.R).sum()),
+                dtype=torch.float64, device=dev)
 
     def run(self, seed=0, stream=None, ssa_fallback_steps=100,
             max_leap_retries=63, step_budget=None, block_size=0):
@@ -169,7 +186,9 @@ class Batch(object):
             o['events'].data_ptr() if 'events' in o else 0,
             o['seqhash'].data_ptr() if 'seqhash' in o else 0,
             o['t_final'].data_ptr() if 't_final' in o else 0,
-            o['score'].data_ptr() if 'score' in o else 0)
+            o['score'].data_ptr() if 'score' in o else 0,
+            o['stats'].data_ptr() if 'stats' in o else 0,
+            o['jacobian'].data_ptr() if 'jacobian' in o else 0)
         r = _lib.RunDesc(0, 0, int(seed) & 0xFFFFFFFFFFFFFFFF, 0, 0,
                          int(ssa_fallback_steps), int(max_leap_retries),
                          int(step_budget), int(block_size), 0)
@@ -183,6 +202,23 @@ class Batch(object):
             'pyst_batch_run')
         return self
 
+    def graph(self, seed=0, **run_kw):
+        """Capture one run of the batch into a CUDA graph and return it
+        (``torch.cuda.CUDAGraph``); ``graph.replay()`` re-runs the whole
+        batch, same seed, with one graph launch.  Runs the batch once
+        uncaptured first (kernel attributes are set outside the capture)."""
+        torch = _torch()
+        self.run(seed=seed, **run_kw)
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                self.run(seed=seed, stream=s, **run_kw)
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        return g
+
     # ---- per-item views -------------------------------------------------
     def samples(self, i):
         a = int(self.sample_offset[i])
@@ -193,6 +229,20 @@ class Batch(object):
     def per_traj(self, name, i):
         a = int(self.traj_offset[i])
         return self.out[name][a:a + int(self.n_traj[i])]
+
+    def stats(self, i):
+        """[kappa, ita, 3]: mean, variance, lag-1 correlation."""
+        a = int(self.stats_offset[i])
+        n = int(self.kappa[i] * self.ita[i] * 3)
+        return self.out['stats'][a:a + n].view(int(self.kappa[i]),
+                                               int(self.ita[i]), 3)
+
+    def jacobian(self, i):
+        """[2, kappa, ita, R]: d mean and d variance by d log rate."""
+        a = int(self.jac_offset[i])
+        n = int(2 * self.kappa[i] * self.ita[i] * self.R[i])
+        return self.out['jacobian'][a:a + n].view(
+            2, int(self.kappa[i]), int(self.ita[i]), int(self.R[i]))
 
     def score(self, i):
         a = int(self.score_offset[i])

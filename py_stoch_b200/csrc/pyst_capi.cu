@@ -92,6 +92,8 @@ OutBase make_outbase(const pyst_outputs* out, int64_t n_traj) {
   ob.seqhash = out->seqhash;
   ob.t_final = out->t_final;
   ob.score = out->score;
+  ob.stats = out->stats;
+  ob.jac = out->jacobian;
   return ob;
 }
 
@@ -112,6 +114,7 @@ int single_run(const uint32_t* h_blob, const uint32_t* d_blob,
   if (!d_workspace || ((uintptr_t)d_workspace & 7)) return PYST_EINVAL;
   if (workspace_bytes < PYST_RUN_WORKSPACE_BYTES) return PYST_EWORKSPACE;
   if (run->n_traj == 0) return PYST_OK;
+  if (out->stats || out->jacobian) return PYST_EINVAL;  // batched runs only
   const RunArgs ra = make_args(run);
   const OutBase ob = make_outbase(out, run->n_traj);
   unsigned long long* queue = (unsigned long long*)d_workspace;
@@ -239,6 +242,7 @@ int pyst_batch_run(const uint32_t* d_blobs, const pyst_batch_item* d_items,
   if (run->step_budget < 0 || run->ssa_fallback_steps < 1 ||
       run->max_leap_retries < 0 || run->max_leap_retries > 63)
     return PYST_EINVAL;
+  if (out->jacobian && !out->score) return PYST_EINVAL;
   if (n_items == 0) return PYST_OK;
   const int bs = run->block_size ? run->block_size : 128;
   if (bs < 32 || bs > 128 || bs % 32) return PYST_EINVAL;

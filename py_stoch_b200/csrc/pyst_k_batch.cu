@@ -14,12 +14,89 @@ namespace pyst {
 // merged at link time; a per-flavour namespace keeps them apart.
 namespace PYST_CAT(batch_flavour_, PYST_SCORE, ) {
 
+// Summary statistics and score Jacobians of one finished item, computed by
+// the block that ran it from the samples (and scores) it just wrote, sums
+// over trajectories in trajectory order.  Means and variances go to shared
+// scratch `ms` when 2*kappa*ita doubles fit, else they are recomputed.
+__device__ void item_epilogue(const ModelView& m, const pyst_batch_item& item,
+                              const OutBase& ob, double* ms, int ms_bytes) {
+  const int ita = m.ita, KF = m.kappa * m.ita, R = m.R;
+  const int64_t U = item.n_traj;
+  if (U <= 0) return;
+  const int32_t* smp = ob.samples + item.sample_offset;
+  const double dU = (double)U;
+  const bool keep = (size_t)KF * 16 <= (size_t)ms_bytes;
+  auto row_moments = [&](int kf, double& mean, double& var) {
+    const int32_t* row = smp + (int64_t)kf * U;
+    double s = 0.0, s2 = 0.0;
+    for (int64_t u = 0; u < U; ++u) {
+      const double x = (double)row[u];
+      s = __dadd_rn(s, x);
+      s2 = __dadd_rn(s2, __dmul_rn(x, x));
+    }
+    mean = __ddiv_rn(s, dU);
+    var = __dsub_rn(__ddiv_rn(s2, dU), __dmul_rn(mean, mean));
+  };
+  for (int kf = threadIdx.x; kf < KF; kf += blockDim.x) {
+    double mean, var;
+    row_moments(kf, mean, var);
+    if (keep) {
+      ms[2 * kf] = mean;
+      ms[2 * kf + 1] = var;
+    }
+    if (ob.stats) {
+      double corr = 0.0;
+      const int f = kf % ita;
+      if (f + 1 < ita) {
+        double mb, vb;
+        row_moments(kf + 1, mb, vb);
+        const int32_t* ra_ = smp + (int64_t)kf * U;
+        const int32_t* rb = ra_ + U;
+        double sab = 0.0;
+        for (int64_t u = 0; u < U; ++u)
+          sab = __dadd_rn(sab, __dmul_rn((double)ra_[u], (double)rb[u]));
+        const double cov = __dsub_rn(__ddiv_rn(sab, dU), __dmul_rn(mean, mb));
+        const double den = __dmul_rn(var, vb);
+        if (den > 0.0) corr = __ddiv_rn(cov, __dsqrt_rn(den));
+      }
+      double* o = ob.stats + item.stats_offset + (int64_t)kf * 3;
+      o[0] = mean;
+      o[1] = var;
+      o[2] = corr;
+    }
+  }
+  if (!ob.jac || !ob.score) return;
+  __syncthreads();
+  const double* sc = ob.score + item.score_offset;
+  for (int idx = threadIdx.x; idx < KF * R; idx += blockDim.x) {
+    const int kf = idx / R, j = idx - kf * R;
+    double mean, var;
+    if (keep) {
+      mean = ms[2 * kf];
+      var = ms[2 * kf + 1];
+    } else {
+      row_moments(kf, mean, var);
+    }
+    const int32_t* row = smp + (int64_t)kf * U;
+    double gm = 0.0, gv = 0.0;
+    for (int64_t u = 0; u < U; ++u) {
+      const double d = __dsub_rn((double)row[u], mean);
+      const double s = sc[u * R + j];
+      gm = __dadd_rn(gm, __dmul_rn(d, s));
+      gv = __dadd_rn(gv, __dmul_rn(__dsub_rn(__dmul_rn(d, d), var), s));
+    }
+    double* o = ob.jac + item.jac_offset;
+    o[(int64_t)kf * R + j] = __ddiv_rn(gm, dU);
+    o[((int64_t)KF + kf) * R + j] = __ddiv_rn(gv, dU);
+  }
+}
+
 template <bool SCORE>
 __global__ void __launch_bounds__(128)
     k_batch(const uint32_t* __restrict__ gblobs,
             const pyst_batch_item* __restrict__ items, int64_t n_items,
             RunArgs ra, OutBase ob, unsigned long long* queue,
-            int max_blob_words, int warp_bytes) {
+            int max_blob_words, int warp_bytes, int dyn_bytes) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ long long s_item;
   uint32_t* sblob = (uint32_t*)smem;
@@ -83,6 +160,10 @@ __global__ void __launch_bounds__(128)
         else run_warp<false, SCORE>(m, ws, ra, id, o, sacc);
       }
     }
+    if (ob.stats || ob.jac) {
+      __syncthreads();  // the item's samples are all written
+      item_epilogue(m, item, ob, (double*)dyn, dyn_bytes);
+    }
     __syncthreads();  // everyone done with sblob and dyn before restaging
   }
 }
@@ -113,7 +194,8 @@ int PYST_CAT(launch_batch_, PYST_SCORE, )(
   int64_t grid = (int64_t)num_sms() * per_sm;
   if (grid > n_items) grid = n_items;
   kf<<<(unsigned)grid, bs, smem, st>>>(d_blobs, d_items, n_items, ra, ob,
-                                       queue, lim->max_blob_words, (int)wb);
+                                       queue, lim->max_blob_words, (int)wb,
+                                       (int)dyn);
   return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
 }
 

@@ -22,6 +22,8 @@ struct OutBase {
   uint64_t* seqhash;
   double* t_final;
   double* score;
+  double* stats;
+  double* jac;
 
   __device__ __forceinline__ TrajOut at(int64_t sample_off, int64_t u,
                                         int64_t traj_off, int64_t score_off,

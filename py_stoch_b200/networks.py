@@ -113,3 +113,34 @@ def synthetic_networks(n_networks, seed=0, s_range=(5, 64), r_range=(8, 256),
         m.name = 'synthetic'
         out.append(m)
     return out
+
+
+LV_NOMINAL = (10.0, 0.01, 10.0)
+
+
+def parameter_sweep(n_sets, seed=1, n_samples=50, lv_t_end=10.0,
+                    schlogl_t_end=5.0):
+    """Parameter sets drawn log-uniformly within one decade of the
+    Lotka-Volterra (k1, k2, k3) and Schlogl (c1..c4; A, B fixed) nominal
+    values, half of each (Lotka-Volterra first), as engine models with
+    n_samples sample times up to t_end = 10 (Lotka-Volterra) / 5 (Schlogl).
+    Returns (models, log_factors): log_factors[i] is the log of the
+    set's rates relative to the nominal ones."""
+    rng = np.random.default_rng(seed)
+    n_lv = n_sets // 2
+    out, logf = [], []
+    for i in range(n_sets):
+        if i < n_lv:
+            f = rng.uniform(-np.log(10), np.log(10), 3)
+            k = np.array(LV_NOMINAL) * np.exp(f)
+            m = lotka_volterra(k1=k[0], k2=k[1], k3=k[2], t_end=lv_t_end,
+                               n_samples=n_samples)
+        else:
+            f = rng.uniform(-np.log(10), np.log(10), 4)
+            c = np.array([SCHLOGL_NOMINAL[n] for n in ('c1', 'c2', 'c3', 'c4')
+                          ]) * np.exp(f)
+            m = schlogl(c1=c[0], c2=c[1], c3=c[2], c4=c[3],
+                        t_end=schlogl_t_end, n_samples=n_samples)
+        out.append(m)
+        logf.append(f)
+    return out, logf

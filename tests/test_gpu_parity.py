@@ -315,3 +315,34 @@ def test_sorted_scheduler_matches_unsorted(torch_cuda, built_lib, oracle_mod,
         np.testing.assert_array_equal(a['score'], b['score'])
     _compare(a, _oracle(oracle_mod, m, n, 'tau', 'thread', seed=8),
              score=score)
+
+
+def test_batch_stats_and_jacobian(torch_cuda, built_lib):
+    """In-kernel per-item statistics and score Jacobians equal the same
+    reductions done in NumPy on the batch's own samples and scores."""
+    from py_stoch_b200.batch import Batch
+    models = [networks.lotka_volterra(t_end=0.5, n_samples=9),
+              networks.schlogl(t_end=1.0, n_samples=12),
+              networks.telegraph(t_end=5.0, n_samples=7)]
+    b = Batch(models, [200, 300, 129], method=['tau', 'tau', 'direct'],
+              score=True, stats=True, jacobian=True)
+    b.run(seed=3)
+    torch_cuda.cuda.synchronize()
+    for i in range(len(models)):
+        x = b.samples(i).cpu().numpy().astype(np.float64)
+        s = b.score(i).cpu().numpy()
+        st = b.stats(i).cpu().numpy()
+        jac = b.jacobian(i).cpu().numpy()
+        m = x.mean(axis=2)
+        v = (x * x).mean(axis=2) - m * m
+        np.testing.assert_allclose(st[..., 0], m, rtol=1e-12)
+        np.testing.assert_allclose(st[..., 1], v, rtol=1e-9, atol=1e-9)
+        cov = (x[:, :-1] * x[:, 1:]).mean(axis=2) - m[:, :-1] * m[:, 1:]
+        den = v[:, :-1] * v[:, 1:]
+        corr = np.where(den > 0, cov / np.sqrt(np.where(den > 0, den, 1)), 0)
+        np.testing.assert_allclose(st[:, :-1, 2], corr, rtol=1e-7, atol=1e-9)
+        d = x - m[..., None]
+        want_m = np.einsum('kfu,uj->kfj', d, s) / x.shape[2]
+        want_v = np.einsum('kfu,uj->kfj', d * d - v[..., None], s) / x.shape[2]
+        np.testing.assert_allclose(jac[0], want_m, rtol=1e-8, atol=1e-8)
+        np.testing.assert_allclose(jac[1], want_v, rtol=1e-8, atol=1e-6)
