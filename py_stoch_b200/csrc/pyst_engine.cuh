@@ -188,6 +188,11 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
 #define SL(i) slot[(int64_t)(i) * bs]
   Stream rs = make_stream(ra.seed, traj_id);
   rs.n = st.n;
+  // The main stream is stateless, so its next block (and that block's
+  // exponential variate) is computed one step ahead, off the dependent
+  // chain of the current step; rs.n runs one block ahead of use.
+  uint4 w_pf = next_block(rs);
+  double e_pf = -pyst_log(u53(w_pf.x, w_pf.y));
   double t = st.t;
   int f = st.f;
   int64_t events = st.events, steps = st.steps;
@@ -285,8 +290,10 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
         double tau2 = __longlong_as_double(0x7ff0000000000000ll);
         uint4 wc = make_uint4(0, 0, 0, 0);
         if (a0c > 0.0) {
-          wc = next_block(rs);
-          tau2 = __ddiv_rn(-pyst_log(u53(wc.x, wc.y)), a0c);
+          wc = w_pf;
+          tau2 = __ddiv_rn(e_pf, a0c);
+          w_pf = next_block(rs);
+          e_pf = -pyst_log(u53(w_pf.x, w_pf.y));
         }
         const double tau1d = (double)tau1;
         double tau = (tau2 < tau1d) ? tau2 : tau1d;
@@ -404,8 +411,10 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
     // ------------------------ one direct-method step -------------------
     steps++;
     n_ssa++;
-    const uint4 w = next_block(rs);
-    const double tau = __ddiv_rn(-pyst_log(u53(w.x, w.y)), a0);
+    const uint4 w = w_pf;
+    const double tau = __ddiv_rn(e_pf, a0);
+    w_pf = next_block(rs);
+    e_pf = -pyst_log(u53(w_pf.x, w_pf.y));
     const double r = __dmul_rn(u53(w.z, w.w), a0);
     int sel = -1;
     {
@@ -471,7 +480,7 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
     }
   }
   st.t = t;
-  st.n = rs.n;
+  st.n = rs.n - 1;  // the prefetched block was not used
   st.events = events;
   st.steps = steps;
   st.h = h;
