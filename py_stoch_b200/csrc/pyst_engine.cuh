@@ -182,7 +182,8 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
                              int bs, const RunArgs& ra, uint64_t traj_id,
                              TState& st, double* integ, int* cnt,
                              const TrajOut& o, int cap_ssa, int cap_leap,
-                             bool stop_on_switch, long long deadline = 0) {
+                             bool stop_on_switch, long long deadline = 0,
+                             int* reached = nullptr, int n_active = 0) {
   const int S = m.S, R = m.R, ita = m.ita, kappa = m.kappa;
 #define XV(i) xcol[(int64_t)(i) * bs]
 #define SL(i) slot[(int64_t)(i) * bs]
@@ -209,8 +210,18 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
   int n_ssa = 0, n_leap = 0;
   auto xget = [&](int i) { return XV(i); };
 
+  bool counted = false;
   while (true) {
-    if (n_ssa >= cap_ssa || n_leap >= cap_leap) break;
+    if (n_ssa >= cap_ssa || n_leap >= cap_leap) {
+      if (!reached) break;
+      // cooperative round end: keep stepping past the cap until every
+      // active thread of the block has reached its own cap or stopped
+      if (!counted) {
+        counted = true;
+        atomicAdd(reached, 1);
+      }
+      if (*(volatile int*)reached >= n_active) break;
+    }
     if (deadline && (long long)clock64() > deadline) break;
     float a[MAXR];
     double a0 = 0.0;
@@ -479,6 +490,7 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
       if (--ssa_left <= 0) ssa_mode = false;
     }
   }
+  if (reached && !counted) atomicAdd(reached, 1);
   st.t = t;
   st.n = rs.n - 1;  // the prefetched block was not used
   st.events = events;
@@ -563,7 +575,8 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
                                  int64_t* slot, int bs, const RunArgs& ra,
                                  uint64_t traj_id, TState& st,
                                  const TrajOut& o, int cap_ssa, int cap_leap,
-                                 bool stop_on_switch) {
+                                 bool stop_on_switch, int* reached = nullptr,
+                                 int n_active = 0) {
   const int S = m.S, R = m.R, ita = m.ita, kappa = m.kappa;
 #define XV(i) xcol[(int64_t)(i) * bs]
 #define SL(i) slot[(int64_t)(i) * bs]
@@ -584,8 +597,16 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
   int n_ssa = 0, n_leap = 0;
   auto xget = [&](int i) { return XV(i); };
 
+  bool counted = false;
   while (true) {
-    if (n_ssa >= cap_ssa || n_leap >= cap_leap) break;
+    if (n_ssa >= cap_ssa || n_leap >= cap_leap) {
+      if (!reached) break;
+      if (!counted) {
+        counted = true;
+        atomicAdd(reached, 1);
+      }
+      if (*(volatile int*)reached >= n_active) break;
+    }
     double a0 = 0.0;
     for (int j = 0; j < R; ++j)
       a0 = __dadd_rn(a0, (double)propensity(m, j, xget));
@@ -800,6 +821,7 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
       if (--ssa_left <= 0) ssa_mode = false;
     }
   }
+  if (reached && !counted) atomicAdd(reached, 1);
   st.t = t;
   st.n = rs.n;
   st.events = events;
@@ -821,15 +843,15 @@ __device__ __forceinline__ void any_round(
     const ModelView& m, int32_t* xcol, int64_t* slot, int bs,
     const RunArgs& ra, uint64_t traj_id, TState& st, double* integ, int* cnt,
     const TrajOut& o, int cap_ssa, int cap_leap, bool stop_on_switch,
-    long long deadline) {
+    long long deadline, int* reached, int n_active) {
   if constexpr (MAXR == 0) {
     static_assert(!SCORE, "the large-R thread engine keeps no scores");
     thread_round_big<TAU>(m, xcol, slot, bs, ra, traj_id, st, o, cap_ssa,
-                          cap_leap, stop_on_switch);
+                          cap_leap, stop_on_switch, reached, n_active);
   } else {
     thread_round<MAXR, TAU, SCORE>(m, xcol, slot, bs, ra, traj_id, st, integ,
                                    cnt, o, cap_ssa, cap_leap, stop_on_switch,
-                                   deadline);
+                                   deadline, reached, n_active);
   }
 }
 
