@@ -37,6 +37,9 @@ constexpr int kBlock = kScore ? 128 : 256;
 // warps do not idle at the regrouping barrier.  Off: on the Schlogl
 // workload it measured 1.48x slower (316 vs 214 ms) -- the warps that keep
 // stepping take issue slots from the slowest warp and stretch the round.
+#ifndef PYST_MIXED_HALF
+#define PYST_MIXED_HALF 1
+#endif
 #ifndef PYST_COOP_ROUNDS
 #define PYST_COOP_ROUNDS 0
 #endif
@@ -166,6 +169,10 @@ __global__ void __launch_bounds__(kBlock, PYST_SORTED_MINB)
   if (tid == 0) s_reached = 0;
   int n_active = __syncthreads_count(active);
 
+  // After sorting, at most one warp per block holds both SSA and leaping
+  // slots and executes both code paths in turn; it runs rounds of half
+  // length so it reaches the regrouping barrier with the pure warps.
+  int my_cap_ssa = cap_ssa, my_cap_leap = cap_leap;
   while (true) {
     if (active) {
       const TrajOut o = ob.at(0, u, 0, 0, ob.stride, R);
@@ -173,7 +180,7 @@ __global__ void __launch_bounds__(kBlock, PYST_SORTED_MINB)
           PYST_ROUND_CYCLES ? (long long)clock64() + PYST_ROUND_CYCLES : 0;
       any_round<MAXR, true, kScore>(m, xa + tid, slotc, kBlock, ra,
                                     id_base + (uint64_t)u, st, integ, cnt, o,
-                                    cap_ssa, cap_leap, true, deadline,
+                                    my_cap_ssa, my_cap_leap, true, deadline,
                                     PYST_COOP_ROUNDS ? &s_reached : nullptr,
                                     n_active);
       if (st.flags & TS_DONE) {
@@ -252,6 +259,15 @@ __global__ void __launch_bounds__(kBlock, PYST_SORTED_MINB)
       }
     }
     active = u >= 0;
+    {
+      const bool in_leap = active && (st.flags & TS_LEAPGRP);
+      const bool in_ssa = active && !(st.flags & TS_LEAPGRP);
+      const bool mixed = PYST_MIXED_HALF &&
+                         __any_sync(0xffffffffu, in_leap) &&
+                         __any_sync(0xffffffffu, in_ssa);
+      my_cap_ssa = mixed ? (cap_ssa + 1) / 2 : cap_ssa;
+      my_cap_leap = mixed ? (cap_leap + 1) / 2 : cap_leap;
+    }
     int32_t* tmp = xa;
     xa = xb;
     xb = tmp;
