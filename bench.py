@@ -42,13 +42,13 @@ def workloads():
             desc='plain cuTauLeaping, Schlogl (c1=3e-7,c2=1e-4,c3=1e-3,'
                  'c4=3.5,A=1e5,B=2e5), X0=250, eps=0.03, n_c=10, 100-step '
                  'SSA fallback, 262144 trajectories, t_end=5, 200 samples',
-            cpu_pilot=1024),
+            cpu_pilot=1024, ref_config='schlogl_tl_262144'),
         'lv_ssa': dict(
             model=networks.lotka_volterra(), n=1024, method='direct',
             desc='plain Gillespie direct method, Lotka-Volterra (k1=10, '
                  'k2=0.01, k3=10), X0=Y0=1000, 1024 trajectories, t_end=10,'
                  ' 100 samples, Philox ids 0..1023',
-            cpu_pilot=64),
+            cpu_pilot=64, ref_config='lv_ssa_1024'),
     }
 
 
@@ -139,10 +139,78 @@ def cpu_baseline(wl, target_s=12.0, threads=0):
             'trajectories_per_s': n / dt}
 
 
+def expected_events(wl, n=2048):
+    """Mean reaction firings per trajectory of the workload, from the CPU
+    oracle (same law as the reference; the reference kernels do not count
+    firings).  Returns (mean, standard error)."""
+    from oracle import oracle
+    m, meth = wl['model'], 0 if wl['method'] == 'direct' else 1
+    r = oracle.simulate(m, n, meth, seed=77)
+    ev = r['events'].astype(np.float64)
+    return ev.mean(), ev.std(ddof=1) / np.sqrt(n)
+
+
+def run_reference_kernels(args, wl):
+    """The reference's own kernels on the GPU (oracle/_ref), replaying
+    CuTauLeaping.run / CuGillespie.run; wall clock per run, since the
+    reference synchronises the host every round."""
+    import torch
+    from oracle import ref_harness
+    r = ref_harness.ReferenceRun(wl['ref_config'])
+    U = r.info['U']
+    for _ in range(args.warmup):
+        O, _ = r.run()
+        O.cpu()
+    times, rounds = [], []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        O, nr = r.run()
+        host = O.cpu()  # CuTauLeaping.run returns O copied to the host
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+        rounds.append(nr)
+    del host
+    mean_ev, se_ev = expected_events(wl)
+    tot = float(np.sum(times))
+    val = mean_ev * U * args.steps / tot
+    line = {'impl': 'reference', 'metric': METRIC, 'value': val,
+            'unit': UNIT, 'n_gpus': args.gpus, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': 1e3 * tot / args.steps,
+            'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f64/f32', 'data': 'synthetic',
+            'config': {'workload': wl['desc']},
+            'trajectories_per_s': U * args.steps / tot,
+            'reference': {'kernels': 'the reference\'s kernel_P1_P2/'
+                          'kernel_P3/init_rng (or kernel_Gillespie) CUDA '
+                          'source, compiled for sm_100a, host loop of '
+                          'CuTauLeaping.run replayed (oracle/ref_harness.py)',
+                          'host_rounds_per_step': float(np.mean(rounds)),
+                          'events_per_trajectory_estimate': mean_ev,
+                          'events_estimate_se': se_ev},
+            'cpu_baseline': {'value': val, 'unit': UNIT, 'cores': 1,
+                             'kind': 'reference',
+                             'sample': 'full workload (%d trajectories) '
+                                       'on the GPU, one host thread '
+                                       'driving it' % U},
+            'e2e': {'value': val, 'unit': UNIT, 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0}}
+    print(json.dumps(line))
+    return 0
+
+
 def run_reference(args, wl):
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return 0
+    try:
+        import torch
+        from oracle import ref_harness
+        if (wl.get('ref_config') and torch.cuda.is_available()
+                and ref_harness.available(wl['ref_config'])):
+            return run_reference_kernels(args, wl)
+    except ImportError:
+        pass
     from oracle import oracle
     m, meth = wl['model'], 0 if wl['method'] == 'direct' else 1
     n = wl['cpu_pilot']
