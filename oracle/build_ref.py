@@ -37,6 +37,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 OUT = os.path.join(HERE, '_ref')
+DEFAULT_REF = '/root/reference'
+
+
+def reference_present(ref=DEFAULT_REF):
+    return os.path.isdir(os.path.join(ref, 'mod'))
 
 # name -> (fixture, species_init, params, output species, t_max, ita, U,
 #          gillespie flag, simulator class)
@@ -102,7 +107,7 @@ def _arr(a):
             'shape': list(a.shape)}
 
 
-def build(ref='/root/reference', names=None):
+def build(ref=DEFAULT_REF, names=None):
     os.makedirs(OUT, exist_ok=True)
     G = _load_golden_module()
     from py_stoch_b200 import sbml as fake_libsbml
@@ -160,5 +165,5 @@ def build(ref='/root/reference', names=None):
 
 if __name__ == '__main__':
     sys.path.insert(0, REPO)
-    build(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    build(sys.argv[1] if len(sys.argv) > 1 else DEFAULT_REF)
     print('built', OUT)

@@ -7,7 +7,7 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if REPO not in sys.path:
     sys.path.insert(0, REPO)
 
-REFERENCE = '/root/reference'
+from oracle.build_ref import DEFAULT_REF as REFERENCE  # noqa: E402
 
 
 def pytest_configure(config):
@@ -39,4 +39,5 @@ def oracle_mod():
 
 
 def reference_available():
-    return os.path.isdir(os.path.join(REFERENCE, 'mod'))
+    from oracle.build_ref import reference_present
+    return reference_present()
