@@ -172,21 +172,20 @@ __device__ __forceinline__ void thread_init(const ModelView& m, int32_t* xcol,
 
 // Advance one trajectory.  Returns when it finishes, or -- for block
 // scheduling -- when it has taken cap_ssa SSA steps or cap_leap leaps in
-// this call, when the SM clock passes `deadline` (if non-zero), or when a
-// DECIDE picks the other mode than the one the call started in
-// (stop_on_switch).  It stops only between steps, so the trajectory resumes
+// this call, or when a DECIDE picks the other mode than the one the call
+// started in (stop_on_switch).  Species counts are xcol[i*bs], the leap
+// scratch of species i is slot[i*ss].  It stops only between steps, so the trajectory resumes
 // exactly where it left off.  With unbounded caps this is the whole
 // trajectory.
 template <int MAXR, bool TAU, bool SCORE>
 __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
-                             int bs, const RunArgs& ra, uint64_t traj_id,
-                             TState& st, double* integ, int* cnt,
-                             const TrajOut& o, int cap_ssa, int cap_leap,
-                             bool stop_on_switch, long long deadline = 0,
-                             int* reached = nullptr, int n_active = 0) {
+                             int bs, int ss, const RunArgs& ra,
+                             uint64_t traj_id, TState& st, double* integ,
+                             int* cnt, const TrajOut& o, int cap_ssa,
+                             int cap_leap, bool stop_on_switch) {
   const int S = m.S, R = m.R, ita = m.ita, kappa = m.kappa;
 #define XV(i) xcol[(int64_t)(i) * bs]
-#define SL(i) slot[(int64_t)(i) * bs]
+#define SL(i) slot[(int64_t)(i) * ss]
   Stream rs = make_stream(ra.seed, traj_id);
   rs.n = st.n;
   // The main stream is stateless, so its next block (and that block's
@@ -210,19 +209,8 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
   int n_ssa = 0, n_leap = 0;
   auto xget = [&](int i) { return XV(i); };
 
-  bool counted = false;
   while (true) {
-    if (n_ssa >= cap_ssa || n_leap >= cap_leap) {
-      if (!reached) break;
-      // cooperative round end: keep stepping past the cap until every
-      // active thread of the block has reached its own cap or stopped
-      if (!counted) {
-        counted = true;
-        atomicAdd(reached, 1);
-      }
-      if (*(volatile int*)reached >= n_active) break;
-    }
-    if (deadline && (long long)clock64() > deadline) break;
+    if (n_ssa >= cap_ssa || n_leap >= cap_leap) break;
     float a[MAXR];
     double a0 = 0.0;
 #pragma unroll
@@ -490,7 +478,6 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
       if (--ssa_left <= 0) ssa_mode = false;
     }
   }
-  if (reached && !counted) atomicAdd(reached, 1);
   st.t = t;
   st.n = rs.n - 1;  // the prefetched block was not used
   st.events = events;
@@ -545,8 +532,9 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
     integ[j] = 0.0;
     cnt[j] = 0;
   }
-  thread_round<MAXR, TAU, SCORE>(m, xcol, slot, bs, ra, traj_id, st, integ,
-                                 cnt, o, 0x7fffffff, 0x7fffffff, false);
+  thread_round<MAXR, TAU, SCORE>(m, xcol, slot, bs, bs, ra, traj_id, st,
+                                 integ, cnt, o, 0x7fffffff, 0x7fffffff,
+                                 false);
   thread_finish<MAXR, SCORE>(m, xcol, bs, st, integ, cnt, o);
 }
 
@@ -572,14 +560,13 @@ __device__ __forceinline__ bool is_critical(const ModelView& m, int j,
 
 template <bool TAU>
 __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
-                                 int64_t* slot, int bs, const RunArgs& ra,
-                                 uint64_t traj_id, TState& st,
-                                 const TrajOut& o, int cap_ssa, int cap_leap,
-                                 bool stop_on_switch, int* reached = nullptr,
-                                 int n_active = 0) {
+                                 int64_t* slot, int bs, int ss,
+                                 const RunArgs& ra, uint64_t traj_id,
+                                 TState& st, const TrajOut& o, int cap_ssa,
+                                 int cap_leap, bool stop_on_switch) {
   const int S = m.S, R = m.R, ita = m.ita, kappa = m.kappa;
 #define XV(i) xcol[(int64_t)(i) * bs]
-#define SL(i) slot[(int64_t)(i) * bs]
+#define SL(i) slot[(int64_t)(i) * ss]
   Stream rs = make_stream(ra.seed, traj_id);
   rs.n = st.n;
   double t = st.t;
@@ -597,16 +584,8 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
   int n_ssa = 0, n_leap = 0;
   auto xget = [&](int i) { return XV(i); };
 
-  bool counted = false;
   while (true) {
-    if (n_ssa >= cap_ssa || n_leap >= cap_leap) {
-      if (!reached) break;
-      if (!counted) {
-        counted = true;
-        atomicAdd(reached, 1);
-      }
-      if (*(volatile int*)reached >= n_active) break;
-    }
+    if (n_ssa >= cap_ssa || n_leap >= cap_leap) break;
     double a0 = 0.0;
     for (int j = 0; j < R; ++j)
       a0 = __dadd_rn(a0, (double)propensity(m, j, xget));
@@ -821,7 +800,6 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
       if (--ssa_left <= 0) ssa_mode = false;
     }
   }
-  if (reached && !counted) atomicAdd(reached, 1);
   st.t = t;
   st.n = rs.n;
   st.events = events;
@@ -840,18 +818,17 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
 // thread_round for MAXR > 0 (register arrays), thread_round_big for 0
 template <int MAXR, bool TAU, bool SCORE>
 __device__ __forceinline__ void any_round(
-    const ModelView& m, int32_t* xcol, int64_t* slot, int bs,
+    const ModelView& m, int32_t* xcol, int64_t* slot, int bs, int ss,
     const RunArgs& ra, uint64_t traj_id, TState& st, double* integ, int* cnt,
-    const TrajOut& o, int cap_ssa, int cap_leap, bool stop_on_switch,
-    long long deadline, int* reached, int n_active) {
+    const TrajOut& o, int cap_ssa, int cap_leap, bool stop_on_switch) {
   if constexpr (MAXR == 0) {
     static_assert(!SCORE, "the large-R thread engine keeps no scores");
-    thread_round_big<TAU>(m, xcol, slot, bs, ra, traj_id, st, o, cap_ssa,
-                          cap_leap, stop_on_switch, reached, n_active);
+    thread_round_big<TAU>(m, xcol, slot, bs, ss, ra, traj_id, st, o, cap_ssa,
+                          cap_leap, stop_on_switch);
   } else {
-    thread_round<MAXR, TAU, SCORE>(m, xcol, slot, bs, ra, traj_id, st, integ,
-                                   cnt, o, cap_ssa, cap_leap, stop_on_switch,
-                                   deadline, reached, n_active);
+    thread_round<MAXR, TAU, SCORE>(m, xcol, slot, bs, ss, ra, traj_id, st,
+                                   integ, cnt, o, cap_ssa, cap_leap,
+                                   stop_on_switch);
   }
 }
 
@@ -861,8 +838,8 @@ __device__ void run_thread_big(const ModelView& m, int32_t* xcol,
                                uint64_t traj_id, const TrajOut& o) {
   TState st;
   thread_init<TAU>(m, xcol, bs, st);
-  thread_round_big<TAU>(m, xcol, slot, bs, ra, traj_id, st, o, 0x7fffffff,
-                        0x7fffffff, false);
+  thread_round_big<TAU>(m, xcol, slot, bs, bs, ra, traj_id, st, o,
+                        0x7fffffff, 0x7fffffff, false);
   thread_finish<1, false>(m, xcol, bs, st, nullptr, nullptr, o);
 }
 

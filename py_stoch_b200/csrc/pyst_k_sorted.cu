@@ -3,14 +3,20 @@
 // In tau-leaping each trajectory is, at any time, either in an SSA
 // fallback round (mod/simulator/cuTauLeaping/P3.py:71-151) or leaping
 // (P1_P2.py:96-297).  The reference runs the two as separate kernels, so in
-// each launch the threads of the other mode sit idle.  Here a block keeps
-// its trajectories' state in shared-memory slots and runs in rounds: every
-// thread advances the trajectory in its slot for up to cap_ssa SSA steps or
-// cap_leap leaps (stopping early when a DECIDE switches mode); between
-// rounds the block refills finished slots from the global work queue and
-// counting-sorts the slots by mode, so each warp executes one kind of step.
-// Per-trajectory arithmetic is exactly that of run_thread, so results do not
-// depend on the schedule.  Built once per PYST_SCORE flavour.
+// each launch the threads of the other mode sit idle.  Here a block keeps a
+// pool of (up to 2) x kBlock trajectory slots in shared memory (species counts
+// and the per-trajectory state between rounds) and runs in rounds: it
+// counting-sorts the occupied slots by mode, picks up to kBlock of them --
+// whole warps of one mode where it can, rotating through each mode's slots
+// so that every trajectory keeps advancing -- and each thread advances the
+// trajectory in its picked slot for up to cap_ssa SSA steps or cap_leap
+// leaps (stopping early when a DECIDE switches mode).  A finished
+// trajectory's slot is refilled from the global work queue.  With more slots
+// than threads every trajectory of a launch that fits the pools starts at
+// once, so no long trajectory starts late, and the mode mix of a round can
+// be chosen from a larger set.  Per-trajectory arithmetic is exactly that of
+// run_thread, so results do not depend on the schedule.  Built once per
+// PYST_SCORE flavour.
 #include "pyst_launch.cuh"
 
 namespace pyst {
@@ -18,259 +24,316 @@ namespace pyst {
 namespace PYST_CAT(sorted_flavour_, PYST_SCORE, ) {
 
 constexpr bool kScore = (bool)PYST_SCORE;
-constexpr int kBlock = kScore ? 128 : 256;
-
-// Blocks per SM the register allocation must allow (launch bounds); 4
-// (at most 64 registers) measured fastest on B200 for the Schlogl
-// workload, ahead of 3 (85) and 1 (unbounded, 111).
+// Threads per block.
+#ifndef PYST_SORTED_BLOCK
+#define PYST_SORTED_BLOCK 512
+#endif
+// Blocks per SM the register allocation must allow (launch bounds): the
+// product with the block size is 1024 threads, at most 64 registers each.
 #ifndef PYST_SORTED_MINB
-#define PYST_SORTED_MINB 4
+#define PYST_SORTED_MINB (1024 / PYST_SORTED_BLOCK)
 #endif
-// Round length in SM clock cycles (0: rounds end only on the step caps).
-// A time box makes the warps of a block reach the regrouping barrier
-// together whatever mix of SSA steps and leaps they run.
-#ifndef PYST_ROUND_CYCLES
-#define PYST_ROUND_CYCLES 0
+// Trajectory slots per thread (the most; the launcher lowers it to 1 when
+// a model's species do not fit twice).
+#ifndef PYST_SORTED_POOL
+#define PYST_SORTED_POOL 2
 #endif
-// Cooperative round end: a thread at its step cap keeps stepping until
-// every active thread of the block has reached its cap or stopped, so
-// warps do not idle at the regrouping barrier.  Off: on the Schlogl
-// workload it measured 1.48x slower (316 vs 214 ms) -- the warps that keep
-// stepping take issue slots from the slowest warp and stretch the round.
+// The one warp per round that holds both SSA and leaping slots runs rounds
+// of half length.
 #ifndef PYST_MIXED_HALF
 #define PYST_MIXED_HALF 1
 #endif
-#ifndef PYST_COOP_ROUNDS
-#define PYST_COOP_ROUNDS 0
-#endif
+constexpr int kBlock = kScore ? 128 : PYST_SORTED_BLOCK;
+constexpr int kMinBlocks = kScore ? 4 : PYST_SORTED_MINB;
+constexpr int kMaxPool = PYST_SORTED_POOL;
+constexpr int kWarps = kBlock / 32;
 
 struct SortedSmem {
   uint32_t* blob;
   uint64_t* bar;
-  int32_t* xa;
-  int32_t* xb;
-  int64_t* slot;
-  double* t;
+  int64_t* scratch;  // [S][kBlock] leap scratch of the running threads
+  double* t;         // per slot [pool * kBlock] ...
   uint64_t* n;
   int64_t* events;
   int64_t* steps;
   uint64_t* h;
-  int64_t* traj;
+  int64_t* traj;     // trajectory index, -1 for an empty slot
+  double* integ;     // [MAXR][slots]
+  int32_t* x;        // [S][slots] species counts
   int32_t* f;
   uint32_t* leap_q;
   int32_t* ssa_left;
   int32_t* flags;
-  double* integ;  // [MAXR][kBlock]
-  int32_t* cnt;   // [MAXR][kBlock]
-  int32_t* wcnt;  // [2][warps]
+  int32_t* cnt;      // [MAXR][slots]
+  int32_t* run;      // [kBlock] slot run by each thread this round
+  int32_t* gcnt;     // [2][pool * kWarps] SSA / leaping slots per 32-group
+  int slots;         // pool * kBlock: the stride of every per-slot array
 };
 
 __host__ __device__ inline size_t sorted_smem_bytes(int blob_words, int S,
-                                                    int maxr) {
+                                                    int maxr, int pool) {
+  const size_t slots = (size_t)pool * kBlock;
   size_t b = (size_t)blob_words * 4 + 16;
-  b += (size_t)S * kBlock * 4 * 2;  // xa, xb
-  b += (size_t)S * kBlock * 8;      // slot
-  b += (size_t)kBlock * (8 * 6 + 4 * 4);
-  if (kScore) b += (size_t)maxr * kBlock * 12;
-  b += 2 * (kBlock / 32) * 4;
+  b += (size_t)S * kBlock * 8;
+  b += slots * (8 * 6 + 4 * 4);
+  b += (size_t)S * slots * 4;
+  if (kScore) b += (size_t)maxr * slots * 12;
+  b += (size_t)kBlock * 4 + 2 * (size_t)pool * kWarps * 4;
   return (b + 15) & ~(size_t)15;
 }
 
 __device__ inline SortedSmem carve(unsigned char* p, int blob_words, int S,
-                                   int maxr) {
+                                   int maxr, int pool) {
   SortedSmem s;
+  const int slots = pool * kBlock;
+  s.slots = slots;
   s.blob = (uint32_t*)p;
   p += (size_t)blob_words * 4;
   s.bar = (uint64_t*)p;
   p += 16;
-  s.slot = (int64_t*)p;
+  s.scratch = (int64_t*)p;
   p += (size_t)S * kBlock * 8;
   s.t = (double*)p;
-  p += kBlock * 8;
+  p += slots * 8;
   s.n = (uint64_t*)p;
-  p += kBlock * 8;
+  p += slots * 8;
   s.events = (int64_t*)p;
-  p += kBlock * 8;
+  p += slots * 8;
   s.steps = (int64_t*)p;
-  p += kBlock * 8;
+  p += slots * 8;
   s.h = (uint64_t*)p;
-  p += kBlock * 8;
+  p += slots * 8;
   s.traj = (int64_t*)p;
-  p += kBlock * 8;
+  p += slots * 8;
   s.integ = (double*)p;
-  if (kScore) p += (size_t)maxr * kBlock * 8;
-  s.xa = (int32_t*)p;
-  p += (size_t)S * kBlock * 4;
-  s.xb = (int32_t*)p;
-  p += (size_t)S * kBlock * 4;
+  if (kScore) p += (size_t)maxr * slots * 8;
+  s.x = (int32_t*)p;
+  p += (size_t)S * slots * 4;
   s.f = (int32_t*)p;
-  p += kBlock * 4;
+  p += slots * 4;
   s.leap_q = (uint32_t*)p;
-  p += kBlock * 4;
+  p += slots * 4;
   s.ssa_left = (int32_t*)p;
-  p += kBlock * 4;
+  p += slots * 4;
   s.flags = (int32_t*)p;
-  p += kBlock * 4;
+  p += slots * 4;
   s.cnt = (int32_t*)p;
-  if (kScore) p += (size_t)maxr * kBlock * 4;
-  s.wcnt = (int32_t*)p;
+  if (kScore) p += (size_t)maxr * slots * 4;
+  s.run = (int32_t*)p;
+  p += kBlock * 4;
+  s.gcnt = (int32_t*)p;
   return s;
 }
 
+__device__ __forceinline__ void load_state(const SortedSmem& s, int p,
+                                           TState& st) {
+  st.t = s.t[p];
+  st.n = s.n[p];
+  st.events = s.events[p];
+  st.steps = s.steps[p];
+  st.h = s.h[p];
+  st.f = s.f[p];
+  st.leap_q = s.leap_q[p];
+  st.ssa_left = s.ssa_left[p];
+  st.flags = s.flags[p];
+}
+
+__device__ __forceinline__ void store_state(const SortedSmem& s, int p,
+                                            const TState& st) {
+  s.t[p] = st.t;
+  s.n[p] = st.n;
+  s.events[p] = st.events;
+  s.steps[p] = st.steps;
+  s.h[p] = st.h;
+  s.f[p] = st.f;
+  s.leap_q[p] = st.leap_q;
+  s.ssa_left[p] = st.ssa_left;
+  s.flags[p] = st.flags;
+}
+
+// Put trajectory u (or nothing, u >= n_traj) into slot p.
+template <int NACC>
+__device__ __forceinline__ void fill_slot(const SortedSmem& s,
+                                          const ModelView& m, int p,
+                                          int64_t u, int64_t n_traj) {
+  if (u < n_traj) {
+    TState st;
+    thread_init<true>(m, s.x + p, s.slots, st);
+    store_state(s, p, st);
+    s.traj[p] = u;
+    if (kScore) {
+#pragma unroll
+      for (int j = 0; j < NACC; ++j) {
+        s.integ[j * s.slots + p] = 0.0;
+        s.cnt[j * s.slots + p] = 0;
+      }
+    }
+  } else {
+    s.traj[p] = -1;
+  }
+}
+
 template <int MAXR>
-__global__ void __launch_bounds__(kBlock, PYST_SORTED_MINB)
+__global__ void __launch_bounds__(kBlock, kMinBlocks)
     k_tau_sorted(const uint32_t* __restrict__ gblob, int blob_words,
                  int64_t n_traj, uint64_t id_base, RunArgs ra, OutBase ob,
-                 unsigned long long* queue, int cap_ssa, int cap_leap) {
+                 unsigned long long* queue, int cap_ssa, int cap_leap,
+                 int pool) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int S = (int)__ldg(gblob + PYST_H_S);
-  SortedSmem sm = carve(smem, blob_words, S, MAXR);
+  SortedSmem sm = carve(smem, blob_words, S, MAXR, pool);
+  const int slots = sm.slots, groups = pool * kWarps;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  constexpr int nw = kBlock / 32;
   if (tid == 0) {
     mbar_init(sm.bar, 1);
     fence_barrier_init();
   }
   __syncthreads();
   const bool ok = stage_blob(sm.blob, gblob, blob_words, sm.bar, 0);
-  const int64_t nthreads = (int64_t)gridDim.x * kBlock;
-  int64_t u = blockIdx.x * (int64_t)kBlock + tid;
+  // Initial fill: a balanced contiguous range per block when every
+  // trajectory fits the pools, else full pools and the queue for the rest.
+  const int64_t grid = gridDim.x;
+  const bool full = n_traj >= grid * slots;
+  const int64_t lo = full ? (int64_t)blockIdx.x * slots
+                          : (int64_t)blockIdx.x * n_traj / grid;
+  const int64_t hi = full ? lo + slots
+                          : ((int64_t)blockIdx.x + 1) * n_traj / grid;
+  const int64_t qbase = full ? grid * slots : n_traj;
   if (!ok) {
     mbar_wait(sm.bar, 0);
+    for (int k = 0; k < pool; ++k) {
+      const int64_t u = lo + k * kBlock + tid;
+      if (u < hi) mark_staging_failure(ob, u);
+    }
+    int64_t u = qbase + (int64_t)atomicAdd(queue, 1ull);
     while (u < n_traj) {
       mark_staging_failure(ob, u);
-      u = nthreads + (int64_t)atomicAdd(queue, 1ull);
+      u = qbase + (int64_t)atomicAdd(queue, 1ull);
     }
     return;
   }
   ModelView m;
   m.load(sm.blob);
   const int R = m.R;
-  int32_t* xa = sm.xa;
-  int32_t* xb = sm.xb;
-  int64_t* slotc = sm.slot + tid;
-  TState st;
   constexpr int kAcc = (kScore && MAXR > 0) ? MAXR : 1;
-  double integ[kAcc];
-  int cnt[kAcc];
-  auto zero_score = [&]() {
-#pragma unroll
-    for (int j = 0; j < kAcc; ++j) {
-      integ[j] = 0.0;
-      cnt[j] = 0;
-    }
-  };
-  bool active = u < n_traj;
-  zero_score();
-  if (active) thread_init<true>(m, xa + tid, kBlock, st);
-  else st.flags = TS_DONE;
+  for (int k = 0; k < pool; ++k) {
+    const int p = k * kBlock + tid;
+    const int64_t u = lo + p;
+    fill_slot<kAcc>(sm, m, p, u < hi ? u : n_traj, n_traj);
+  }
   const unsigned lt = (1u << lane) - 1u;
-  __shared__ int s_reached;
-  if (tid == 0) s_reached = 0;
-  int n_active = __syncthreads_count(active);
+  int rot0 = 0, rot1 = 0;
+  __syncthreads();
 
-  // After sorting, at most one warp per block holds both SSA and leaping
-  // slots and executes both code paths in turn; it runs rounds of half
-  // length so it reaches the regrouping barrier with the pure warps.
-  int my_cap_ssa = cap_ssa, my_cap_leap = cap_leap;
   while (true) {
-    if (active) {
-      const TrajOut o = ob.at(0, u, 0, 0, ob.stride, R);
-      const long long deadline =
-          PYST_ROUND_CYCLES ? (long long)clock64() + PYST_ROUND_CYCLES : 0;
-      any_round<MAXR, true, kScore>(m, xa + tid, slotc, kBlock, ra,
-                                    id_base + (uint64_t)u, st, integ, cnt, o,
-                                    my_cap_ssa, my_cap_leap, true, deadline,
-                                    PYST_COOP_ROUNDS ? &s_reached : nullptr,
-                                    n_active);
-      if (st.flags & TS_DONE) {
-        thread_finish<(MAXR > 0 ? MAXR : 1), kScore>(m, xa + tid, kBlock, st,
-                                                     integ, cnt, o);
-        u = nthreads + (int64_t)atomicAdd(queue, 1ull);
-        active = u < n_traj;
-        zero_score();
-        if (active) thread_init<true>(m, xa + tid, kBlock, st);
+    // ---- schedule: counting sort of the slots by (SSA, leap, empty) ----
+    int key[kMaxPool];
+    unsigned b0[kMaxPool], b1[kMaxPool];
+#pragma unroll
+    for (int k = 0; k < kMaxPool; ++k) {
+      if (k >= pool) break;
+      const int p = k * kBlock + tid;
+      key[k] = sm.traj[p] < 0 ? 2 : ((sm.flags[p] & TS_LEAPGRP) ? 1 : 0);
+      b0[k] = __ballot_sync(0xffffffffu, key[k] == 0);
+      b1[k] = __ballot_sync(0xffffffffu, key[k] == 1);
+      if (lane == 0) {
+        sm.gcnt[k * kWarps + wid] = __popc(b0[k]);
+        sm.gcnt[groups + k * kWarps + wid] = __popc(b1[k]);
       }
-    }
-    // ---- regroup: counting sort of the slots by (SSA, leap, empty) ----
-    const int key = !active ? 2 : ((st.flags & TS_LEAPGRP) ? 1 : 0);
-    const unsigned b0 = __ballot_sync(0xffffffffu, key == 0);
-    const unsigned b1 = __ballot_sync(0xffffffffu, key == 1);
-    if (lane == 0) {
-      sm.wcnt[wid] = __popc(b0);
-      sm.wcnt[nw + wid] = __popc(b1);
     }
     __syncthreads();
-    int tot0 = 0, tot1 = 0, pre0 = 0, pre1 = 0, pre2 = 0;
+    int tot0 = 0, tot1 = 0, pre0[kMaxPool], pre1[kMaxPool];
 #pragma unroll
-    for (int w = 0; w < nw; ++w) {
-      const int c0 = sm.wcnt[w], c1 = sm.wcnt[nw + w];
-      tot0 += c0;
-      tot1 += c1;
-      if (w < wid) {
-        pre0 += c0;
-        pre1 += c1;
-        pre2 += 32 - c0 - c1;
+    for (int k = 0; k < kMaxPool; ++k) pre0[k] = pre1[k] = 0;
+    for (int g = 0; g < groups; ++g) {
+#pragma unroll
+      for (int k = 0; k < kMaxPool; ++k) {
+        if (g == k * kWarps + wid) {
+          pre0[k] = tot0;
+          pre1[k] = tot1;
+        }
       }
+      tot0 += sm.gcnt[g];
+      tot1 += sm.gcnt[groups + g];
     }
     if (tot0 + tot1 == 0) break;  // uniform: every thread read the same
-    n_active = tot0 + tot1;
-    if (tid == 0) s_reached = 0;  // read only after the next barrier
-    int rank;
-    if (key == 0) rank = pre0 + __popc(b0 & lt);
-    else if (key == 1) rank = tot0 + pre1 + __popc(b1 & lt);
-    else rank = tot0 + tot1 + pre2 + __popc(~(b0 | b1) & lt);
-    // move this slot's state to position `rank`
-    sm.t[rank] = st.t;
-    sm.n[rank] = st.n;
-    sm.events[rank] = st.events;
-    sm.steps[rank] = st.steps;
-    sm.h[rank] = st.h;
-    sm.traj[rank] = active ? u : -1;
-    sm.f[rank] = st.f;
-    sm.leap_q[rank] = st.leap_q;
-    sm.ssa_left[rank] = st.ssa_left;
-    sm.flags[rank] = st.flags;
-    for (int i = 0; i < S; ++i)
-      xb[(int64_t)i * kBlock + rank] = xa[(int64_t)i * kBlock + tid];
-    if (kScore) {
+    // how many slots of each mode run: all if they fit, else a split in
+    // proportion to the counts, in whole warps, with at least one warp's
+    // worth of a mode that has any slots
+    int n0 = tot0, n1 = tot1;
+    if (tot0 + tot1 > kBlock) {
+      n0 = (int)(((int64_t)tot0 * kBlock / (tot0 + tot1) + 16) / 32 * 32);
+      const int min0 = tot0 < 32 ? tot0 : 32;
+      const int min1 = tot1 < 32 ? tot1 : 32;
+      if (n0 < min0) n0 = min0;
+      if (n0 > kBlock - min1) n0 = kBlock - min1;
+      if (n0 > tot0) n0 = tot0;
+      n1 = kBlock - n0;
+      if (n1 > tot1) {
+        n1 = tot1;
+        n0 = kBlock - n1;
+      }
+    }
+    if (tot0) rot0 %= tot0;
+    if (tot1) rot1 %= tot1;
+#pragma unroll
+    for (int k = 0; k < kMaxPool; ++k) {
+      if (k >= pool) break;
+      const int p = k * kBlock + tid;
+      if (key[k] == 0) {
+        int pos = pre0[k] + __popc(b0[k] & lt) - rot0;
+        if (pos < 0) pos += tot0;
+        if (pos < n0) sm.run[pos] = p;
+      } else if (key[k] == 1) {
+        int pos = pre1[k] + __popc(b1[k] & lt) - rot1;
+        if (pos < 0) pos += tot1;
+        if (pos < n1) sm.run[n0 + pos] = p;
+      }
+    }
+    rot0 += n0;
+    rot1 += n1;
+    __syncthreads();
+    // ---- run ----
+    const int nrun = n0 + n1;
+    if (tid < nrun) {
+      const int p = sm.run[tid];
+      // the warp holding both modes (n0 inside it) runs half-length rounds
+      const bool mixed = PYST_MIXED_HALF && n0 > wid * 32 &&
+                         n0 < wid * 32 + 32 && nrun > n0;
+      const int my_cap_ssa = mixed ? (cap_ssa + 1) / 2 : cap_ssa;
+      const int my_cap_leap = mixed ? (cap_leap + 1) / 2 : cap_leap;
+      TState st;
+      load_state(sm, p, st);
+      double integ[kAcc];
+      int cnt[kAcc];
 #pragma unroll
       for (int j = 0; j < kAcc; ++j) {
-        sm.integ[j * kBlock + rank] = integ[j];
-        sm.cnt[j * kBlock + rank] = cnt[j];
+        integ[j] = kScore ? sm.integ[j * slots + p] : 0.0;
+        cnt[j] = kScore ? sm.cnt[j * slots + p] : 0;
+      }
+      const int64_t u = sm.traj[p];
+      const TrajOut o = ob.at(0, u, 0, 0, ob.stride, R);
+      any_round<MAXR, true, kScore>(m, sm.x + p, sm.scratch + tid, slots,
+                                    kBlock, ra, id_base + (uint64_t)u, st,
+                                    integ, cnt, o, my_cap_ssa, my_cap_leap,
+                                    true);
+      if (st.flags & TS_DONE) {
+        thread_finish<(MAXR > 0 ? MAXR : 1), kScore>(m, sm.x + p, slots, st,
+                                                     integ, cnt, o);
+        fill_slot<kAcc>(sm, m, p, qbase + (int64_t)atomicAdd(queue, 1ull),
+                        n_traj);
+      } else {
+        store_state(sm, p, st);
+        if (kScore) {
+#pragma unroll
+          for (int j = 0; j < kAcc; ++j) {
+            sm.integ[j * slots + p] = integ[j];
+            sm.cnt[j * slots + p] = cnt[j];
+          }
+        }
       }
     }
     __syncthreads();
-    st.t = sm.t[tid];
-    st.n = sm.n[tid];
-    st.events = sm.events[tid];
-    st.steps = sm.steps[tid];
-    st.h = sm.h[tid];
-    u = sm.traj[tid];
-    st.f = sm.f[tid];
-    st.leap_q = sm.leap_q[tid];
-    st.ssa_left = sm.ssa_left[tid];
-    st.flags = sm.flags[tid];
-    if (kScore) {
-#pragma unroll
-      for (int j = 0; j < kAcc; ++j) {
-        integ[j] = sm.integ[j * kBlock + tid];
-        cnt[j] = sm.cnt[j * kBlock + tid];
-      }
-    }
-    active = u >= 0;
-    {
-      const bool in_leap = active && (st.flags & TS_LEAPGRP);
-      const bool in_ssa = active && !(st.flags & TS_LEAPGRP);
-      const bool mixed = PYST_MIXED_HALF &&
-                         __any_sync(0xffffffffu, in_leap) &&
-                         __any_sync(0xffffffffu, in_ssa);
-      my_cap_ssa = mixed ? (cap_ssa + 1) / 2 : cap_ssa;
-      my_cap_leap = mixed ? (cap_leap + 1) / 2 : cap_leap;
-    }
-    int32_t* tmp = xa;
-    xa = xb;
-    xb = tmp;
   }
 }
 
@@ -279,7 +342,12 @@ int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
                uint64_t id_base, const RunArgs& ra, const OutBase& ob,
                unsigned long long* queue, cudaStream_t st, int cap_ssa,
                int cap_leap) {
-  const size_t smem = sorted_smem_bytes(mi.words, mi.S, MR > 0 ? MR : 1);
+  const int maxr = MR > 0 ? MR : 1;
+  int pool = kMaxPool;
+  while (pool > 1 && sorted_smem_bytes(mi.words, mi.S, maxr, pool) >
+                         kMaxDynSmem)
+    --pool;
+  const size_t smem = sorted_smem_bytes(mi.words, mi.S, maxr, pool);
   if (smem > kMaxDynSmem) return PYST_EUNSUPPORTED;
   auto kf = k_tau_sorted<MR>;
   const int rc = set_smem(kf, smem);
@@ -290,11 +358,14 @@ int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf, kBlock, smem);
   if (per_sm < 1) per_sm = 1;
-  int64_t grid = (n + kBlock - 1) / kBlock;
+  // every resident block slot of the GPU, each with at least two warps'
+  // worth of trajectories
+  int64_t grid = (n + 63) / 64;
   const int64_t cap = (int64_t)num_sms() * per_sm;
   if (grid > cap) grid = cap;
   kf<<<(unsigned)grid, kBlock, smem, st>>>(d_blob, mi.words, n, id_base, ra,
-                                           ob, queue, cap_ssa, cap_leap);
+                                           ob, queue, cap_ssa, cap_leap,
+                                           pool);
   return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
 }
 
