@@ -31,12 +31,14 @@ using namespace pyst;
 namespace {
 
 // Round lengths of the mode-sorted tau-leaping kernel: SSA steps and leaps
-// a trajectory advances between two regroupings of its block.
+// a trajectory advances between two regroupings of its block (16 leaps
+// measured 10% faster than 32 on the Schlogl workload, 256 SSA steps as
+// fast as 128 and faster than 512).
 #ifndef PYST_CAP_SSA
 #define PYST_CAP_SSA 256
 #endif
 #ifndef PYST_CAP_LEAP
-#define PYST_CAP_LEAP 32
+#define PYST_CAP_LEAP 16
 #endif
 constexpr int kSortedCapSsa = PYST_CAP_SSA;
 constexpr int kSortedCapLeap = PYST_CAP_LEAP;

@@ -4,9 +4,9 @@
 // fallback round (mod/simulator/cuTauLeaping/P3.py:71-151) or leaping
 // (P1_P2.py:96-297).  The reference runs the two as separate kernels, so in
 // each launch the threads of the other mode sit idle.  Here a block keeps a
-// pool of (up to 2) x kBlock trajectory slots in shared memory (species counts
-// and the per-trajectory state between rounds) and runs in rounds: it
-// counting-sorts the occupied slots by mode, picks up to kBlock of them --
+// pool of (up to 2) x blockDim trajectory slots in shared memory (species
+// counts and the per-trajectory state between rounds) and runs in rounds: it
+// counting-sorts the occupied slots by mode, picks up to blockDim of them --
 // whole warps of one mode where it can, rotating through each mode's slots
 // so that every trajectory keeps advancing -- and each thread advances the
 // trajectory in its picked slot for up to cap_ssa SSA steps or cap_leap
@@ -24,17 +24,17 @@ namespace pyst {
 namespace PYST_CAT(sorted_flavour_, PYST_SCORE, ) {
 
 constexpr bool kScore = (bool)PYST_SCORE;
-// Threads per block.
+// Largest block (threads) and the register budget: 1024 threads per SM at
+// most 64 registers each; the score flavour keeps 128-thread blocks with 4
+// resident (its accumulators need the registers).
+constexpr int kMaxBlock = kScore ? 128 : 1024;
+constexpr int kMinBlocks = kScore ? 4 : 1;
+// Preferred block size: the launcher takes the largest size up to this
+// whose shared memory fits, first with PYST_SORTED_POOL slots per thread,
+// then with one.
 #ifndef PYST_SORTED_BLOCK
-#define PYST_SORTED_BLOCK 512
+#define PYST_SORTED_BLOCK 1024
 #endif
-// Blocks per SM the register allocation must allow (launch bounds): the
-// product with the block size is 1024 threads, at most 64 registers each.
-#ifndef PYST_SORTED_MINB
-#define PYST_SORTED_MINB (1024 / PYST_SORTED_BLOCK)
-#endif
-// Trajectory slots per thread (the most; the launcher lowers it to 1 when
-// a model's species do not fit twice).
 #ifndef PYST_SORTED_POOL
 #define PYST_SORTED_POOL 2
 #endif
@@ -43,16 +43,15 @@ constexpr bool kScore = (bool)PYST_SCORE;
 #ifndef PYST_MIXED_HALF
 #define PYST_MIXED_HALF 1
 #endif
-constexpr int kBlock = kScore ? 128 : PYST_SORTED_BLOCK;
-constexpr int kMinBlocks = kScore ? 4 : PYST_SORTED_MINB;
 constexpr int kMaxPool = PYST_SORTED_POOL;
-constexpr int kWarps = kBlock / 32;
+constexpr int kPrefBlock =
+    PYST_SORTED_BLOCK < kMaxBlock ? PYST_SORTED_BLOCK : kMaxBlock;
 
 struct SortedSmem {
   uint32_t* blob;
   uint64_t* bar;
-  int64_t* scratch;  // [S][kBlock] leap scratch of the running threads
-  double* t;         // per slot [pool * kBlock] ...
+  int64_t* scratch;  // [S][block] leap scratch of the running threads
+  double* t;         // per slot [pool * block] ...
   uint64_t* n;
   int64_t* events;
   int64_t* steps;
@@ -65,34 +64,35 @@ struct SortedSmem {
   int32_t* ssa_left;
   int32_t* flags;
   int32_t* cnt;      // [MAXR][slots]
-  int32_t* run;      // [kBlock] slot run by each thread this round
-  int32_t* gcnt;     // [2][pool * kWarps] SSA / leaping slots per 32-group
-  int slots;         // pool * kBlock: the stride of every per-slot array
+  int32_t* run;      // [block] slot run by each thread this round
+  int32_t* gcnt;     // [2][pool * block / 32] SSA / leaping slots per group
+  int slots;         // pool * block: the stride of every per-slot array
 };
 
 __host__ __device__ inline size_t sorted_smem_bytes(int blob_words, int S,
-                                                    int maxr, int pool) {
-  const size_t slots = (size_t)pool * kBlock;
+                                                    int maxr, int pool,
+                                                    int block) {
+  const size_t slots = (size_t)pool * block;
   size_t b = (size_t)blob_words * 4 + 16;
-  b += (size_t)S * kBlock * 8;
+  b += (size_t)S * block * 8;
   b += slots * (8 * 6 + 4 * 4);
   b += (size_t)S * slots * 4;
   if (kScore) b += (size_t)maxr * slots * 12;
-  b += (size_t)kBlock * 4 + 2 * (size_t)pool * kWarps * 4;
+  b += (size_t)block * 4 + 2 * (size_t)pool * (block / 32) * 4;
   return (b + 15) & ~(size_t)15;
 }
 
 __device__ inline SortedSmem carve(unsigned char* p, int blob_words, int S,
-                                   int maxr, int pool) {
+                                   int maxr, int pool, int block) {
   SortedSmem s;
-  const int slots = pool * kBlock;
+  const int slots = pool * block;
   s.slots = slots;
   s.blob = (uint32_t*)p;
   p += (size_t)blob_words * 4;
   s.bar = (uint64_t*)p;
   p += 16;
   s.scratch = (int64_t*)p;
-  p += (size_t)S * kBlock * 8;
+  p += (size_t)S * block * 8;
   s.t = (double*)p;
   p += slots * 8;
   s.n = (uint64_t*)p;
@@ -120,7 +120,7 @@ __device__ inline SortedSmem carve(unsigned char* p, int blob_words, int S,
   s.cnt = (int32_t*)p;
   if (kScore) p += (size_t)maxr * slots * 4;
   s.run = (int32_t*)p;
-  p += kBlock * 4;
+  p += block * 4;
   s.gcnt = (int32_t*)p;
   return s;
 }
@@ -174,15 +174,16 @@ __device__ __forceinline__ void fill_slot(const SortedSmem& s,
 }
 
 template <int MAXR>
-__global__ void __launch_bounds__(kBlock, kMinBlocks)
+__global__ void __launch_bounds__(kMaxBlock, kMinBlocks)
     k_tau_sorted(const uint32_t* __restrict__ gblob, int blob_words,
                  int64_t n_traj, uint64_t id_base, RunArgs ra, OutBase ob,
                  unsigned long long* queue, int cap_ssa, int cap_leap,
                  int pool) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int S = (int)__ldg(gblob + PYST_H_S);
-  SortedSmem sm = carve(smem, blob_words, S, MAXR, pool);
-  const int slots = sm.slots, groups = pool * kWarps;
+  const int nb = blockDim.x, nw = nb >> 5;
+  SortedSmem sm = carve(smem, blob_words, S, MAXR, pool, nb);
+  const int slots = sm.slots, groups = pool * nw;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   if (tid == 0) {
     mbar_init(sm.bar, 1);
@@ -202,7 +203,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
   if (!ok) {
     mbar_wait(sm.bar, 0);
     for (int k = 0; k < pool; ++k) {
-      const int64_t u = lo + k * kBlock + tid;
+      const int64_t u = lo + k * nb + tid;
       if (u < hi) mark_staging_failure(ob, u);
     }
     int64_t u = qbase + (int64_t)atomicAdd(queue, 1ull);
@@ -217,7 +218,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
   const int R = m.R;
   constexpr int kAcc = (kScore && MAXR > 0) ? MAXR : 1;
   for (int k = 0; k < pool; ++k) {
-    const int p = k * kBlock + tid;
+    const int p = k * nb + tid;
     const int64_t u = lo + p;
     fill_slot<kAcc>(sm, m, p, u < hi ? u : n_traj, n_traj);
   }
@@ -232,13 +233,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
 #pragma unroll
     for (int k = 0; k < kMaxPool; ++k) {
       if (k >= pool) break;
-      const int p = k * kBlock + tid;
+      const int p = k * nb + tid;
       key[k] = sm.traj[p] < 0 ? 2 : ((sm.flags[p] & TS_LEAPGRP) ? 1 : 0);
       b0[k] = __ballot_sync(0xffffffffu, key[k] == 0);
       b1[k] = __ballot_sync(0xffffffffu, key[k] == 1);
       if (lane == 0) {
-        sm.gcnt[k * kWarps + wid] = __popc(b0[k]);
-        sm.gcnt[groups + k * kWarps + wid] = __popc(b1[k]);
+        sm.gcnt[k * nw + wid] = __popc(b0[k]);
+        sm.gcnt[groups + k * nw + wid] = __popc(b1[k]);
       }
     }
     __syncthreads();
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     for (int g = 0; g < groups; ++g) {
 #pragma unroll
       for (int k = 0; k < kMaxPool; ++k) {
-        if (g == k * kWarps + wid) {
+        if (g == k * nw + wid) {
           pre0[k] = tot0;
           pre1[k] = tot1;
         }
@@ -261,17 +262,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     // proportion to the counts, in whole warps, with at least one warp's
     // worth of a mode that has any slots
     int n0 = tot0, n1 = tot1;
-    if (tot0 + tot1 > kBlock) {
-      n0 = (int)(((int64_t)tot0 * kBlock / (tot0 + tot1) + 16) / 32 * 32);
+    if (tot0 + tot1 > nb) {
+      n0 = (int)(((int64_t)tot0 * nb / (tot0 + tot1) + 16) / 32 * 32);
       const int min0 = tot0 < 32 ? tot0 : 32;
       const int min1 = tot1 < 32 ? tot1 : 32;
       if (n0 < min0) n0 = min0;
-      if (n0 > kBlock - min1) n0 = kBlock - min1;
+      if (n0 > nb - min1) n0 = nb - min1;
       if (n0 > tot0) n0 = tot0;
-      n1 = kBlock - n0;
+      n1 = nb - n0;
       if (n1 > tot1) {
         n1 = tot1;
-        n0 = kBlock - n1;
+        n0 = nb - n1;
       }
     }
     if (tot0) rot0 %= tot0;
@@ -279,7 +280,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
 #pragma unroll
     for (int k = 0; k < kMaxPool; ++k) {
       if (k >= pool) break;
-      const int p = k * kBlock + tid;
+      const int p = k * nb + tid;
       if (key[k] == 0) {
         int pos = pre0[k] + __popc(b0[k] & lt) - rot0;
         if (pos < 0) pos += tot0;
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
       const int64_t u = sm.traj[p];
       const TrajOut o = ob.at(0, u, 0, 0, ob.stride, R);
       any_round<MAXR, true, kScore>(m, sm.x + p, sm.scratch + tid, slots,
-                                    kBlock, ra, id_base + (uint64_t)u, st,
+                                    nb, ra, id_base + (uint64_t)u, st,
                                     integ, cnt, o, my_cap_ssa, my_cap_leap,
                                     true);
       if (st.flags & TS_DONE) {
@@ -343,12 +344,17 @@ int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
                unsigned long long* queue, cudaStream_t st, int cap_ssa,
                int cap_leap) {
   const int maxr = MR > 0 ? MR : 1;
-  int pool = kMaxPool;
-  while (pool > 1 && sorted_smem_bytes(mi.words, mi.S, maxr, pool) >
-                         kMaxDynSmem)
-    --pool;
-  const size_t smem = sorted_smem_bytes(mi.words, mi.S, maxr, pool);
-  if (smem > kMaxDynSmem) return PYST_EUNSUPPORTED;
+  // the largest block up to the preferred size whose pools fit, first with
+  // kMaxPool slots per thread, then with one
+  int pool = 0, block = 0;
+  for (int p = kMaxPool; p >= 1 && !block; --p)
+    for (int b = kPrefBlock; b >= 64 && !block; b >>= 1)
+      if (sorted_smem_bytes(mi.words, mi.S, maxr, p, b) <= kMaxDynSmem) {
+        pool = p;
+        block = b;
+      }
+  if (!block) return PYST_EUNSUPPORTED;
+  const size_t smem = sorted_smem_bytes(mi.words, mi.S, maxr, pool, block);
   auto kf = k_tau_sorted<MR>;
   const int rc = set_smem(kf, smem);
   if (rc) return rc;
@@ -356,16 +362,15 @@ int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
       cudaSuccess)
     return PYST_ECUDA;
   int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf, kBlock, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kf, block, smem);
   if (per_sm < 1) per_sm = 1;
   // every resident block slot of the GPU, each with at least two warps'
   // worth of trajectories
   int64_t grid = (n + 63) / 64;
   const int64_t cap = (int64_t)num_sms() * per_sm;
   if (grid > cap) grid = cap;
-  kf<<<(unsigned)grid, kBlock, smem, st>>>(d_blob, mi.words, n, id_base, ra,
-                                           ob, queue, cap_ssa, cap_leap,
-                                           pool);
+  kf<<<(unsigned)grid, block, smem, st>>>(d_blob, mi.words, n, id_base, ra,
+                                          ob, queue, cap_ssa, cap_leap, pool);
   return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
 }
 
