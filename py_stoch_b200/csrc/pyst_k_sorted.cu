@@ -173,7 +173,8 @@ __device__ __forceinline__ void fill_slot(const SortedSmem& s,
   }
 }
 
-template <int MAXR>
+// NB: block size fixed at compile time, or 0 for blockDim.x.
+template <int MAXR, int NB>
 __global__ void __launch_bounds__(kMaxBlock, kMinBlocks)
     k_tau_sorted(const uint32_t* __restrict__ gblob, int blob_words,
                  int64_t n_traj, uint64_t id_base, RunArgs ra, OutBase ob,
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(kMaxBlock, kMinBlocks)
                  int pool) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int S = (int)__ldg(gblob + PYST_H_S);
-  const int nb = blockDim.x, nw = nb >> 5;
+  const int nb = NB ? NB : blockDim.x, nw = nb >> 5;
   SortedSmem sm = carve(smem, blob_words, S, MAXR, pool, nb);
   const int slots = sm.slots, groups = pool * nw;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -355,7 +356,8 @@ int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
       }
   if (!block) return PYST_EUNSUPPORTED;
   const size_t smem = sorted_smem_bytes(mi.words, mi.S, maxr, pool, block);
-  auto kf = k_tau_sorted<MR>;
+  auto kf = block == kMaxBlock ? k_tau_sorted<MR, kMaxBlock>
+                               : k_tau_sorted<MR, 0>;
   const int rc = set_smem(kf, smem);
   if (rc) return rc;
   if (cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st) !=
