@@ -42,13 +42,27 @@ def workloads():
             desc='plain cuTauLeaping, Schlogl (c1=3e-7,c2=1e-4,c3=1e-3,'
                  'c4=3.5,A=1e5,B=2e5), X0=250, eps=0.03, n_c=10, 100-step '
                  'SSA fallback, 262144 trajectories, t_end=5, 200 samples',
-            cpu_pilot=1024, ref_config='schlogl_tl_262144'),
+            cpu_pilot=1024, ref_config='schlogl_tl_262144',
+            # from one ncu capture of the simulation kernel on 229,376
+            # trajectories (profiles/k_tau_sorted_schlogl_229376.md):
+            # DRAM read + write per trajectory, and warp instructions per
+            # reaction event
+            dram_bytes_per_traj=(666.8e6 + 2165.6e6) / 229376,
+            warp_inst_per_event=45736461188 / 4209068063),
         'lv_ssa': dict(
             model=networks.lotka_volterra(), n=1024, method='direct',
             desc='plain Gillespie direct method, Lotka-Volterra (k1=10, '
                  'k2=0.01, k3=10), X0=Y0=1000, 1024 trajectories, t_end=10,'
                  ' 100 samples, Philox ids 0..1023',
             cpu_pilot=64, ref_config='lv_ssa_1024'),
+        'telegraph_grad': dict(
+            model=networks.telegraph(), n=1048576, method='direct', grad=True,
+            desc='adjoint gradient: telegraph gene expression (k_on=0.5, '
+                 'k_off=0.2, 20, 1, 5, 0.1), gene off, 1048576 direct-method'
+                 ' trajectories with likelihood-ratio scores, t_end=50, 20 '
+                 'samples of protein; step = forward kernel + moments + '
+                 'score-backward reduction of d(mean+var)/d log k',
+            cpu_pilot=256, ref_config=None),
     }
 
 
@@ -262,6 +276,13 @@ def _events_timed(fn, stream):
     return st.elapsed_time(en), out
 
 
+def completed_events(events, status):
+    """Firings of the trajectories that reached t_end or absorption (status
+    DONE / ABSORBED): a leap count of a trajectory that grows until int32
+    overflow or runs out of step budget is not throughput."""
+    return float(events[status <= 1].sum().item())
+
+
 def batch_vs_plain(kind, dev, subset=256, steps=1, full=True, budget=20000):
     """Events/s of the batched form (one persistent launch, CUDA graph) and
     of the plain form (one launch per model) on the same models.
@@ -305,45 +326,52 @@ def batch_vs_plain(kind, dev, subset=256, steps=1, full=True, budget=20000):
                   traj_id_base=ids)
         g = b.graph(seed=11, step_budget=budget)
         g.replay()
-        tot_ms, ev = 0.0, 0.0
+        tot_ms, ev, ev_ok = 0.0, 0.0, 0.0
         for _ in range(steps):
             ms_, _ = _events_timed(g.replay, stream)
             tot_ms += ms_
             ev += float(b.out['events'].sum().item())
+            ev_ok += completed_events(b.out['events'], b.out['status'])
         st = torch.bincount(b.out['status'].long(), minlength=7).tolist()
         del g
-        return tot_ms / steps, ev / steps, st, b
+        return tot_ms / steps, ev / steps, st, b, ev_ok / steps
 
     ids = [i * n_traj for i in pick]
-    ms_b, ev_b, st_b, _ = batched(sub, ids)
+    ms_b, ev_b, st_b, _, ok_b = batched(sub, ids)
     # plain form: one simulate() launch per model, same ids and budget
     outs = [{'samples': torch.empty((m.kappa, m.ita, n_traj),
                                     dtype=torch.int32, device=dev),
-             'events': torch.empty(n_traj, dtype=torch.int64, device=dev)}
+             'events': torch.empty(n_traj, dtype=torch.int64, device=dev),
+             'status': torch.empty(n_traj, dtype=torch.uint8, device=dev)}
             for m in sub]
 
     def plain():
         for k, (m, i) in enumerate(zip(sub, pick)):
             simulate(m, n_traj, method='tau', seed=11,
                      traj_id_base=i * n_traj, device=dev, stream=stream,
-                     out=outs[k], score=grad, status=False,
+                     out=outs[k], score=grad, status=True,
                      step_budget=budget,
                      mapping=('thread' if tuner.mapping(m, 'tau') == 1
                               else 'warp'))
     plain()
     ms_p, _ = _events_timed(plain, stream)
     ev_p = float(sum(int(o['events'].sum().item()) for o in outs))
+    ok_p = sum(completed_events(o['events'], o['status']) for o in outs)
     res['plain'] = {'ms': ms_p, 'events': ev_p, 'events_per_s':
-                    ev_p / ms_p * 1e3, 'launches': len(sub)}
+                    ev_p / ms_p * 1e3, 'completed_events_per_s':
+                    ok_p / ms_p * 1e3, 'launches': len(sub)}
     res['batched_same_models'] = {'ms': ms_b, 'events': ev_b,
                                   'events_per_s': ev_b / ms_b * 1e3,
+                                  'completed_events_per_s':
+                                      ok_b / ms_b * 1e3,
                                   'launches': 1, 'status_counts': st_b}
     res['batched_over_plain'] = (ev_b / ms_b) / (ev_p / ms_p)
     if full:
-        ms_f, ev_f, st_f, b = batched(models)
+        ms_f, ev_f, st_f, b, ok_f = batched(models)
         res['batched_full'] = {'models': len(models), 'ms': ms_f,
                                'events': ev_f,
                                'events_per_s': ev_f / ms_f * 1e3,
+                               'completed_events_per_s': ok_f / ms_f * 1e3,
                                'trajectories_per_s':
                                    len(models) * n_traj / ms_f * 1e3,
                                'status_counts': st_f}
@@ -400,10 +428,23 @@ def main():
                                   device=dev),
            'status': torch.empty(n, dtype=torch.uint8, device=dev),
            'events': torch.empty(n, dtype=torch.int64, device=dev)}
+    grad = bool(wl.get('grad'))
+    if grad:
+        from py_stoch_b200.autograd import _moments, score_backward
+        out['score'] = torch.empty((n, m.n_reactions), dtype=torch.float64,
+                                   device=dev)
+        ones = torch.ones((m.kappa, m.ita), dtype=torch.float64, device=dev)
 
-    def step(seed):
-        return simulate(m, n, method=meth, seed=seed, traj_id_base=base,
-                        device=dev, stream=stream, out=out)
+    def step(seed, d_blob=None):
+        res = simulate(m, n, method=meth, seed=seed, traj_id_base=base,
+                       device=dev, stream=stream, out=out, score=grad,
+                       d_blob=d_blob)
+        if grad:
+            # backward of mean + var of every sample: the score reduction
+            mean, var = _moments(res['samples'])
+            res['grad'] = score_backward(res['samples'], res['score'], mean,
+                                         var, ones, ones, stream=stream)
+        return res
 
     for w in range(args.warmup):
         step(10_000 + w)
@@ -447,6 +488,8 @@ def main():
     d_blob = torch.empty_like(blob, device=dev)
     h_out = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
              for k, v in out.items()}
+    h_grad = torch.empty(m.n_reactions, dtype=torch.float64,
+                         pin_memory=True)
     e2e_ms, e2e_ev = 0.0, 0
     for s in range(args.steps):
         flush.fill_(s & 0xFF)
@@ -454,10 +497,11 @@ def main():
             enable_timing=True)
         st.record(stream)
         d_blob.copy_(blob, non_blocking=True)
-        res = simulate(m, n, method=meth, seed=100 + s, traj_id_base=base,
-                       device=dev, stream=stream, out=out, d_blob=d_blob)
+        res = step(100 + s, d_blob=d_blob)
         for k in h_out:
             h_out[k].copy_(out[k], non_blocking=True)
+        if grad:
+            h_grad.copy_(res['grad'], non_blocking=True)
         en.record(stream)
         en.synchronize()
         e2e_ms += st.elapsed_time(en)
@@ -471,12 +515,28 @@ def main():
     e2e_value = float(e2[1]) / (float(e2[0]) / 1e3)
     h2d = blob.numel() * 4
     d2h = sum(v.numel() * v.element_size() for v in h_out.values())
+    if grad:
+        d2h += h_grad.numel() * 8
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
         out_bytes = sum(v.numel() * v.element_size() for v in out.values())
         per_launch_s = sec / args.steps / 1.0
         achieved = out_bytes / per_launch_s / 1e9
+        traffic = (wl['dram_bytes_per_traj'] * n
+                   if 'dram_bytes_per_traj' in wl else None)
+        issue = None
+        if 'warp_inst_per_event' in wl and clocks.get('sm_mhz'):
+            # instruction-issue roofline: warp instructions per second
+            # against 4 schedulers per SM at the sampled SM clock
+            sms = torch.cuda.get_device_properties(dev).multi_processor_count
+            a = value / world * wl['warp_inst_per_event'] / 1e12
+            pk = sms * 4 * clocks['sm_mhz'] * 1e6 / 1e12
+            issue = {'bound': 'issue', 'achieved': a, 'peak': pk,
+                     'unit': 'T warp-inst/s', 'frac': a / pk,
+                     'warp_inst_per_event': wl['warp_inst_per_event'],
+                     'source': 'ncu instruction count per event x measured '
+                               'events/s; peak 4 issue slots/SM/cycle'}
         line = {
             'metric': METRIC, 'value': value, 'unit': UNIT,
             'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
@@ -489,14 +549,21 @@ def main():
             'trajectories_per_s': n * world * args.steps / sec,
             'events_per_step': events / args.steps,
             'error_trajectories': int(errs),
-            'gpu_launches': args.steps,
+            # this library's kernels in the timed region: the simulation,
+            # plus the two-kernel score reduction of the gradient form
+            'gpu_launches': args.steps * (3 if grad else 1),
             'e2e': {'value': e2e_value, 'unit': UNIT,
                     'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak,
                          'unit': 'GB/s', 'frac': achieved / peak,
-                         'traffic': None, 'peak_source': peak_kind,
+                         'traffic': traffic, 'peak_source': peak_kind,
+                         'algorithmic_bytes': out_bytes,
                          'note': 'the kernel is CUDA-core issue bound; HBM '
-                                 'carries only the sample output'},
+                                 'carries only the sample output (traffic: '
+                                 'partially written 32-byte sectors of the '
+                                 '[kappa][ita][U] layout, scaled from a '
+                                 '229376-trajectory ncu capture)'},
+            'issue': issue,
             'clocks': clocks,
         }
         if not args.no_cpu_baseline and world == 1:
@@ -511,7 +578,8 @@ def main():
 
 def forms_main(args):
     """--workload sweep | synthetic: the batched-vs-plain comparison as the
-    JSON line (value = batched events/s over all models)."""
+    JSON line (value = batched events/s over all models, counting the
+    trajectories that completed; all firings in `all_events_per_s`)."""
     import torch
     from py_stoch_b200 import build as _build
     dev = torch.device('cuda', int(os.environ.get('LOCAL_RANK', '0')))
@@ -519,7 +587,8 @@ def forms_main(args):
     _build.build()
     r = batch_vs_plain(args.workload, dev, steps=args.steps, full=True)
     full = r['batched_full']
-    line = {'metric': METRIC, 'value': full['events_per_s'], 'unit': UNIT,
+    line = {'metric': METRIC, 'value': full['completed_events_per_s'],
+            'all_events_per_s': full['events_per_s'], 'unit': UNIT,
             'n_gpus': 1, 'steps': args.steps, 'warmup': 1,
             'ms_per_step': full['ms'], 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32/f64',
