@@ -121,6 +121,71 @@ __device__ __forceinline__ float propensity(const ModelView& m, int j,
   return a;
 }
 
+// Packed reaction descriptors for small mass-action reactions, built in
+// shared memory by each block after staging the model:
+//   factors  pk[j]:     two slots of 13 bits, slot s at bit 13s:
+//                       species (10 bits) | order 1..3 (2 bits) | falling
+//                       (1 bit); order 0 = empty slot;
+//   net      pk[R + j]: two slots of 15 bits, slot s at bit 15s: species
+//                       (10 bits) | delta (5-bit two's complement), and the
+//                       number of entries in bits 30-31.
+// A reaction fits when it has at most two reactant entries of order <= 3
+// and at most two net-change entries with |delta| <= 15 over species
+// < 1024.  The packed forms take the same operations in the same order as
+// the entry lists, so results are identical; they only remove the chains
+// of dependent shared-memory loads (entry pointer -> entry -> species).
+// All threads of the block call this; true when every reaction fits.
+__device__ __forceinline__ bool pack_reactions(const ModelView& m,
+                                               uint32_t* pk) {
+  bool ok = true;
+  for (int j = threadIdx.x; j < m.R; j += blockDim.x) {
+    const int e0 = m.facptr(j), e1 = m.facptr(j + 1);
+    uint32_t d = 0;
+    if (e1 - e0 > 2) ok = false;
+    for (int e = e0; e < e1 && e < e0 + 2; ++e) {
+      const uint32_t fe = m.fac(e);
+      const int sp = ent_lo(fe), n = fac_order(fe);
+      if (sp > 1023 || n < 1 || n > 3) ok = false;
+      d |= ((uint32_t)(sp & 1023) | ((uint32_t)(n & 3) << 10) |
+            ((uint32_t)fac_falling(fe) << 12))
+           << (13 * (e - e0));
+    }
+    pk[j] = d;
+    const int n0 = m.netptr(j), n1 = m.netptr(j + 1);
+    uint32_t q = (uint32_t)(n1 - n0) << 30;
+    if (n1 - n0 > 2) ok = false;
+    for (int e = n0; e < n1 && e < n0 + 2; ++e) {
+      const uint32_t ne = m.net(e);
+      const int sp = ent_lo(ne), v = ent_hi_s16(ne);
+      if (sp > 1023 || v < -16 || v > 15) ok = false;
+      q |= ((uint32_t)(sp & 1023) | ((uint32_t)(v & 31) << 10))
+           << (15 * (e - n0));
+    }
+    pk[m.R + j] = q;
+  }
+  return ok;
+}
+
+// propensity() from a packed factor descriptor and the rate.
+template <class XGet>
+__device__ __forceinline__ float propensity_packed(float rate, uint32_t d,
+                                                   XGet xget) {
+  float a = rate;
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const uint32_t f = d >> (13 * s);
+    const int n = (int)((f >> 10) & 3u);
+    if (n) {
+      const int x = xget((int)(f & 1023u));
+      const int fall = (int)((f >> 12) & 1u);
+      a = __fmul_rn(a, (float)x);
+      if (n > 1) a = __fmul_rn(a, (float)(x - fall));
+      if (n > 2) a = __fmul_rn(a, (float)(x - 2 * fall));
+    }
+  }
+  return a;
+}
+
 __device__ __forceinline__ void store_sample(const TrajOut& o, int ita, int k,
                                              int f, int32_t v) {
   o.samples[((int64_t)k * ita + f) * o.stride] = v;
@@ -201,6 +266,7 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
   bool fill_state = false, done = false;
   const int64_t budget = ra.step_budget;
   const double t_end = m.time(ita - 1);
+  double tf = m.time(f);  // next sample time (f < ita while running)
   bool ssa_mode = (st.flags & TS_SSA) != 0;
   const bool group_leap = (st.flags & TS_LEAPGRP) != 0;
   bool leap_grp = group_leap;
@@ -216,7 +282,8 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
 #pragma unroll
     for (int j = 0; j < MAXR; ++j) {
       if (j >= R) break;
-      a[j] = propensity(m, j, xget);
+      a[j] = m.fast ? propensity_packed(m.rate(j), m.pk[j], xget)
+                    : propensity(m, j, xget);
       a0 = __dadd_rn(a0, (double)a[j]);
     }
     if (a0 == 0.0) {
@@ -387,8 +454,8 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
             integ[j] = __dadd_rn(integ[j], __dmul_rn((double)a[j], tau));
           }
         }
-        while (tn >= m.time(f)) {
-          const double frac = __ddiv_rn(__dsub_rn(m.time(f), t), tau);
+        while (tn >= tf) {
+          const double frac = __ddiv_rn(__dsub_rn(tf, t), tau);
           for (int k = 0; k < kappa; ++k) {
             const int i = m.out(k);
             const double inc = rint(__dmul_rn((double)SL(i), frac));
@@ -399,6 +466,7 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
             done = true;
             break;
           }
+          tf = m.time(f);
         }
         for (int i = 0; i < S; ++i) XV(i) = (int)((int64_t)XV(i) + SL(i));
         events += fired;
@@ -442,25 +510,42 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
         integ[j] = __dadd_rn(integ[j], __dmul_rn((double)a[j], dt));
       }
     }
-    while (tn >= m.time(f)) {
+    while (tn >= tf) {
       for (int k = 0; k < kappa; ++k) store_sample(o, ita, k, f, XV(m.out(k)));
       f++;
       if (f == ita) {
         done = true;
         break;
       }
+      tf = m.time(f);
     }
     t = tn;
     if (done) break;
     {
-      const int e1 = m.netptr(sel + 1);
       bool over = false;
-      for (int e = m.netptr(sel); e < e1; ++e) {
-        const uint32_t ne = m.net(e);
-        const int sp = ent_lo(ne);
-        const int64_t nx = (int64_t)XV(sp) + ent_hi_s16(ne);
-        if (nx < 0 || nx > PYST_I32MAX) over = true;
-        else XV(sp) = (int)nx;
+      if (m.fast) {
+        const uint32_t d = m.pk[R + sel];
+        const int ne = (int)(d >> 30);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          if (q < ne) {
+            const uint32_t f15 = d >> (15 * q);
+            const int sp = (int)(f15 & 1023u);
+            const int dv = ((int)((f15 >> 10) & 31u) ^ 16) - 16;
+            const int64_t nx = (int64_t)XV(sp) + dv;
+            if (nx < 0 || nx > PYST_I32MAX) over = true;
+            else XV(sp) = (int)nx;
+          }
+        }
+      } else {
+        const int e1 = m.netptr(sel + 1);
+        for (int e = m.netptr(sel); e < e1; ++e) {
+          const uint32_t ne = m.net(e);
+          const int sp = ent_lo(ne);
+          const int64_t nx = (int64_t)XV(sp) + ent_hi_s16(ne);
+          if (nx < 0 || nx > PYST_I32MAX) over = true;
+          else XV(sp) = (int)nx;
+        }
       }
       if (over) {
         status = PYST_TRAJ_OVERFLOW;

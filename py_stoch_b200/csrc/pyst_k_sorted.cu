@@ -50,6 +50,7 @@ constexpr int kPrefBlock =
 struct SortedSmem {
   uint32_t* blob;
   uint64_t* bar;
+  uint32_t* pk;      // [2 * maxr] packed reaction descriptors
   int64_t* scratch;  // [S][block] leap scratch of the running threads
   double* t;         // per slot [pool * block] ...
   uint64_t* n;
@@ -73,7 +74,7 @@ __host__ __device__ inline size_t sorted_smem_bytes(int blob_words, int S,
                                                     int maxr, int pool,
                                                     int block) {
   const size_t slots = (size_t)pool * block;
-  size_t b = (size_t)blob_words * 4 + 16;
+  size_t b = (size_t)blob_words * 4 + 16 + packed_bytes(maxr);
   b += (size_t)S * block * 8;
   b += slots * (8 * 6 + 4 * 4);
   b += (size_t)S * slots * 4;
@@ -91,6 +92,8 @@ __device__ inline SortedSmem carve(unsigned char* p, int blob_words, int S,
   p += (size_t)blob_words * 4;
   s.bar = (uint64_t*)p;
   p += 16;
+  s.pk = (uint32_t*)p;
+  p += packed_bytes(maxr);
   s.scratch = (int64_t*)p;
   p += (size_t)S * block * 8;
   s.t = (double*)p;
@@ -217,6 +220,10 @@ __global__ void __launch_bounds__(kMaxBlock, kMinBlocks)
   ModelView m;
   m.load(sm.blob);
   const int R = m.R;
+  if (MAXR > 0) {
+    m.pk = sm.pk;
+    m.fast = __syncthreads_and(pack_reactions(m, sm.pk)) != 0;
+  }
   constexpr int kAcc = (kScore && MAXR > 0) ? MAXR : 1;
   for (int k = 0; k < pool; ++k) {
     const int p = k * nb + tid;

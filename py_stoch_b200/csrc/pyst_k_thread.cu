@@ -26,7 +26,12 @@ __global__ void __launch_bounds__(128)
   extern __shared__ __align__(16) unsigned char smem[];
   uint32_t* sblob = (uint32_t*)smem;
   uint64_t* bar = (uint64_t*)(smem + (size_t)blob_words * 4);
-  int32_t* xbase = (int32_t*)(smem + (size_t)blob_words * 4 + 16);
+  // packed reaction descriptors (register-array engine only), then the
+  // species columns
+  const int R = (int)__ldg(gblob + PYST_H_R);
+  uint32_t* pk = (uint32_t*)(smem + (size_t)blob_words * 4 + 16);
+  int32_t* xbase =
+      (int32_t*)((unsigned char*)pk + (MAXR > 0 ? packed_bytes(R) : 0));
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
     fence_barrier_init();
@@ -48,6 +53,10 @@ __global__ void __launch_bounds__(128)
   }
   ModelView m;
   m.load(sblob);
+  if (MAXR > 0) {
+    m.pk = pk;
+    m.fast = __syncthreads_and(pack_reactions(m, pk)) != 0;
+  }
   int32_t* xcol = xbase + threadIdx.x;
   int64_t* slot = (int64_t*)(xbase + (size_t)m.S * bs) + threadIdx.x;
   while (u < n_traj) {
@@ -87,7 +96,9 @@ int PYST_CAT(launch_plain_thread_, PYST_TAU, PYST_SCORE)(
     uint64_t id_base, const RunArgs& ra, const OutBase& ob, int bs,
     unsigned long long* queue, cudaStream_t st) {
   const size_t smem =
-      (size_t)mi.words * 4 + 16 + (size_t)bs * mi.S * (PYST_TAU ? 12 : 4);
+      (size_t)mi.words * 4 + 16 +
+      (maxr <= PYST_THREAD_MAX_REACTIONS ? packed_bytes(mi.R) : 0) +
+      (size_t)bs * mi.S * (PYST_TAU ? 12 : 4);
   if (smem > kMaxDynSmem) return PYST_EUNSUPPORTED;
   if (n <= 0) return PYST_OK;
   if (cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st) !=

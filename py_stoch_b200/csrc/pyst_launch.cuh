@@ -52,6 +52,12 @@ struct HostModelInfo {
 
 constexpr size_t kMaxDynSmem = 227 * 1024;
 
+// Shared memory of the packed reaction descriptors (pack_reactions): 2R
+// words, rounded up to 16 bytes.
+__host__ __device__ inline size_t packed_bytes(int R) {
+  return ((size_t)R * 8 + 15) & ~(size_t)15;
+}
+
 inline size_t host_warp_bytes(int S, int R, bool score) {
   size_t b = (size_t)S * 8 + (size_t)S * 4 + (size_t)R * 4 + (size_t)R * 4 +
              (((size_t)R + 3) & ~(size_t)3);

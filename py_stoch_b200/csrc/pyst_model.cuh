@@ -22,6 +22,10 @@ struct ModelView {
   int n_c;
   float eta;
   double t_max;
+  // Packed per-reaction descriptors (see pack_reactions), valid when
+  // `fast`: factors of reaction j at pk[j], net changes at pk[R + j].
+  const uint32_t* pk;
+  bool fast;
 
   __device__ __forceinline__ void load(const uint32_t* base) {
     w = base;
@@ -47,6 +51,8 @@ struct ModelView {
     const uint64_t tb = (uint64_t)w[PYST_H_TMAX_LO] |
                         ((uint64_t)w[PYST_H_TMAX_HI] << 32);
     t_max = __longlong_as_double((long long)tb);
+    pk = nullptr;
+    fast = false;
   }
   __device__ __forceinline__ float rate(int j) const {
     return __uint_as_float(w[o_rate + j]);
@@ -151,8 +157,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 
 // Stage `words` (multiple of 4) words of `src` into `dst` with one
 // bulk-async copy issued by thread 0; every thread of the block waits on
-// phase `parity` of `bar`.  Returns false on timeout.  Must be called by all
-// threads of the block.  `bar` must have been initialised with count 1.
+// phase `parity` of `bar`.  Returns false on timeout, the same value in
+// every thread (a block-wide vote, so callers may branch on it around
+// barriers).  Must be called by all threads of the block.  `bar` must have
+// been initialised with count 1.
 __device__ __forceinline__ bool stage_blob(uint32_t* dst, const uint32_t* src,
                                            int words, uint64_t* bar,
                                            uint32_t parity) {
@@ -163,7 +171,7 @@ __device__ __forceinline__ bool stage_blob(uint32_t* dst, const uint32_t* src,
     mbar_arrive_expect_tx(bar, bytes);
     bulk_g2s(dst, src, bytes, bar);
   }
-  return mbar_wait(bar, parity);
+  return __syncthreads_and(mbar_wait(bar, parity)) != 0;
 }
 
 }  // namespace pyst
