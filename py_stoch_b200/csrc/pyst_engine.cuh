@@ -186,6 +186,15 @@ __device__ __forceinline__ float propensity_packed(float rate, uint32_t d,
   return a;
 }
 
+// Entry q (< 2) of a packed net-change descriptor: species and delta.
+__device__ __forceinline__ int pnet_species(uint32_t d, int q) {
+  return (int)((d >> (15 * q)) & 1023u);
+}
+__device__ __forceinline__ int pnet_delta(uint32_t d, int q) {
+  return ((int)((d >> (15 * q + 10)) & 31u) ^ 16) - 16;
+}
+__device__ __forceinline__ int pnet_count(uint32_t d) { return (int)(d >> 30); }
+
 __device__ __forceinline__ void store_sample(const TrajOut& o, int ita, int k,
                                              int f, int32_t v) {
   o.samples[((int64_t)k * ita + f) * o.stride] = v;
@@ -303,11 +312,23 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
 #pragma unroll
       for (int j = 0; j < MAXR; ++j) {
         if (j >= R) break;
-        const int e1 = m.critptr(j + 1);
-        for (int e = m.critptr(j); e < e1; ++e) {
-          const uint32_t ce = m.crit(e);
-          if ((int64_t)(ce >> 16) * m.n_c > (int64_t)XV(ent_lo(ce)))
-            crit |= 1u << j;
+        if (m.fast) {
+          // the negative entries of the net change (same test, any order)
+          const uint32_t d = m.pk[R + j];
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const int v = pnet_delta(d, q);
+            if (q < pnet_count(d) && v < 0 &&
+                (int64_t)(-v) * m.n_c > (int64_t)XV(pnet_species(d, q)))
+              crit |= 1u << j;
+          }
+        } else {
+          const int e1 = m.critptr(j + 1);
+          for (int e = m.critptr(j); e < e1; ++e) {
+            const uint32_t ce = m.crit(e);
+            if ((int64_t)(ce >> 16) * m.n_c > (int64_t)XV(ent_lo(ce)))
+              crit |= 1u << j;
+          }
         }
       }
       for (int i = 0; i < S; ++i) SL(i) = 0;
@@ -315,15 +336,23 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
       for (int j = 0; j < MAXR; ++j) {
         if (j >= R) break;
         if (!((crit >> j) & 1u)) {
-          const int e1 = m.netptr(j + 1);
-          for (int e = m.netptr(j); e < e1; ++e) {
-            const uint32_t ne = m.net(e);
-            const int sp = ent_lo(ne);
-            const int v = ent_hi_s16(ne);
+          auto acc = [&](int sp, int v) {
             float2 ms = *reinterpret_cast<float2*>(&SL(sp));
             ms.x = __fadd_rn(ms.x, __fmul_rn((float)v, a[j]));
             ms.y = __fadd_rn(ms.y, __fmul_rn((float)(v * v), a[j]));
             *reinterpret_cast<float2*>(&SL(sp)) = ms;
+          };
+          if (m.fast) {
+            const uint32_t d = m.pk[R + j];
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+              if (q < pnet_count(d)) acc(pnet_species(d, q), pnet_delta(d, q));
+          } else {
+            const int e1 = m.netptr(j + 1);
+            for (int e = m.netptr(j); e < e1; ++e) {
+              const uint32_t ne = m.net(e);
+              acc(ent_lo(ne), ent_hi_s16(ne));
+            }
           }
         }
       }
@@ -408,10 +437,18 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
           for (int j = 0; j < MAXR; ++j) {
             if (j >= R) break;
             if (K[j] != 0) {
-              const int e1 = m.netptr(j + 1);
-              for (int e = m.netptr(j); e < e1; ++e) {
-                const uint32_t ne = m.net(e);
-                SL(ent_lo(ne)) += (int64_t)K[j] * ent_hi_s16(ne);
+              if (m.fast) {
+                const uint32_t d = m.pk[R + j];
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+                  if (q < pnet_count(d))
+                    SL(pnet_species(d, q)) += (int64_t)K[j] * pnet_delta(d, q);
+              } else {
+                const int e1 = m.netptr(j + 1);
+                for (int e = m.netptr(j); e < e1; ++e) {
+                  const uint32_t ne = m.net(e);
+                  SL(ent_lo(ne)) += (int64_t)K[j] * ent_hi_s16(ne);
+                }
               }
             }
           }
@@ -525,14 +562,11 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
       bool over = false;
       if (m.fast) {
         const uint32_t d = m.pk[R + sel];
-        const int ne = (int)(d >> 30);
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-          if (q < ne) {
-            const uint32_t f15 = d >> (15 * q);
-            const int sp = (int)(f15 & 1023u);
-            const int dv = ((int)((f15 >> 10) & 31u) ^ 16) - 16;
-            const int64_t nx = (int64_t)XV(sp) + dv;
+          if (q < pnet_count(d)) {
+            const int sp = pnet_species(d, q);
+            const int64_t nx = (int64_t)XV(sp) + pnet_delta(d, q);
             if (nx < 0 || nx > PYST_I32MAX) over = true;
             else XV(sp) = (int)nx;
           }

@@ -186,6 +186,17 @@ __device__ __forceinline__ double pyst_logfact(double k) {
 #define PYST_INVERSION_MAX_K 200
 #define PYST_PTRS_MAX_IT 64
 
+// 1/k for k = 1..PYST_INVERSION_MAX_K, correctly rounded (the compiler
+// divides at compile time in IEEE double), so the inversion search reads
+// the value __drcp_rn((double)k) would compute.
+struct PystRcpTable {
+  double v[PYST_INVERSION_MAX_K + 1];
+  constexpr PystRcpTable() : v() {
+    for (int k = 1; k <= PYST_INVERSION_MAX_K; ++k) v[k] = 1.0 / (double)k;
+  }
+};
+__device__ __constant__ PystRcpTable c_rcp = PystRcpTable();
+
 // Counter of the blocks one Poisson draw may use: words (c0, c1 | blk, c2,
 // c3) for blk = 0, 1, ... < 32, key (k0, k1).  The leap sampler sets
 // c0 = leap index, c1 = 0x80000000 | reaction << 12 | retry << 6, (c2, c3)
@@ -216,19 +227,21 @@ static __device__ __noinline__ int poisson(float lam, const PoissonKey& pk) {
     while (u > F && k < PYST_INVERSION_MAX_K) {
       k++;
       // p_k = p_{k-1} * lam * (1/k); 1/k correctly rounded
-      p = __dmul_rn(__dmul_rn(p, l), __drcp_rn((double)k));
+      p = __dmul_rn(__dmul_rn(p, l), c_rcp.v[k]);
       F = __dadd_rn(F, p);
     }
     return k;
   }
   const float slam = __fsqrt_rn(lam);
-  const double loglam = pyst_log((double)lam);
   const float b = __fadd_rn(0.931f, __fmul_rn(2.53f, slam));
   const float a = __fadd_rn(-0.059f, __fmul_rn(0.02483f, b));
   const float invalpha =
       __fadd_rn(1.1239f, __fdiv_rn(1.1328f, __fsub_rn(b, 3.4f)));
   const float vr = __fsub_rn(0.9277f, __fdiv_rn(3.6224f, __fsub_rn(b, 2.0f)));
-  const double log_invalpha = pyst_log((double)invalpha);
+  // the two logs of the exact test, computed when a draw first needs it
+  // (most draws are accepted by the squeeze above it)
+  double loglam = 0.0, log_invalpha = 0.0;
+  bool have_logs = false;
   uint4 w = make_uint4(0, 0, 0, 0);
   for (int it = 0; it < PYST_PTRS_MAX_IT; ++it) {
     uint32_t wu, wv;
@@ -252,6 +265,11 @@ static __device__ __noinline__ int poisson(float lam, const PoissonKey& pk) {
     if (us >= 0.07f && V <= vr) return (int)kf;
     if (kf < 0.0f || (us < 0.013f && V > us)) continue;
     const float den = __fadd_rn(__fdiv_rn(a, __fmul_rn(us, us)), b);
+    if (!have_logs) {
+      loglam = pyst_log((double)lam);
+      log_invalpha = pyst_log((double)invalpha);
+      have_logs = true;
+    }
     double lhs = __dadd_rn(pyst_log((double)V), log_invalpha);
     lhs = __dsub_rn(lhs, pyst_log((double)den));
     const double kd = (double)kf;
