@@ -251,13 +251,20 @@ __device__ __forceinline__ void thread_init(const ModelView& m, int32_t* xcol,
 // scratch of species i is slot[i*ss].  It stops only between steps, so the trajectory resumes
 // exactly where it left off.  With unbounded caps this is the whole
 // trajectory.
-template <int MAXR, bool TAU, bool SCORE>
+// PK: how reactions are read -- kPkLists (entry lists), kPkPacked (packed
+// descriptors, m.fast must hold) or kPkRuntime (whichever m.fast says).
+// The fixed forms carry only their own code and live registers (faster for
+// the plain kernels); the mode-sorted kernel measured faster with one
+// run-time form.
+enum { kPkLists = 0, kPkPacked = 1, kPkRuntime = 2 };
+template <int MAXR, bool TAU, bool SCORE, int PK>
 __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
                              int bs, int ss, const RunArgs& ra,
                              uint64_t traj_id, TState& st, double* integ,
                              int* cnt, const TrajOut& o, int cap_ssa,
                              int cap_leap, bool stop_on_switch) {
   const int S = m.S, R = m.R, ita = m.ita, kappa = m.kappa;
+  const bool pk = PK == kPkPacked || (PK == kPkRuntime && m.fast);
 #define XV(i) xcol[(int64_t)(i) * bs]
 #define SL(i) slot[(int64_t)(i) * ss]
   Stream rs = make_stream(ra.seed, traj_id);
@@ -291,7 +298,7 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
 #pragma unroll
     for (int j = 0; j < MAXR; ++j) {
       if (j >= R) break;
-      a[j] = m.fast ? propensity_packed(m.rate(j), m.pk[j], xget)
+      a[j] = pk ? propensity_packed(m.rate(j), m.pk[j], xget)
                     : propensity(m, j, xget);
       a0 = __dadd_rn(a0, (double)a[j]);
     }
@@ -312,7 +319,7 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
 #pragma unroll
       for (int j = 0; j < MAXR; ++j) {
         if (j >= R) break;
-        if (m.fast) {
+        if (pk) {
           // the negative entries of the net change (same test, any order)
           const uint32_t d = m.pk[R + j];
 #pragma unroll
@@ -342,7 +349,7 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
             ms.y = __fadd_rn(ms.y, __fmul_rn((float)(v * v), a[j]));
             *reinterpret_cast<float2*>(&SL(sp)) = ms;
           };
-          if (m.fast) {
+          if (pk) {
             const uint32_t d = m.pk[R + j];
 #pragma unroll
             for (int q = 0; q < 2; ++q)
@@ -437,7 +444,7 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
           for (int j = 0; j < MAXR; ++j) {
             if (j >= R) break;
             if (K[j] != 0) {
-              if (m.fast) {
+              if (pk) {
                 const uint32_t d = m.pk[R + j];
 #pragma unroll
                 for (int q = 0; q < 2; ++q)
@@ -560,7 +567,7 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
     if (done) break;
     {
       bool over = false;
-      if (m.fast) {
+      if (pk) {
         const uint32_t d = m.pk[R + sel];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
@@ -651,9 +658,14 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
     integ[j] = 0.0;
     cnt[j] = 0;
   }
-  thread_round<MAXR, TAU, SCORE>(m, xcol, slot, bs, bs, ra, traj_id, st,
-                                 integ, cnt, o, 0x7fffffff, 0x7fffffff,
-                                 false);
+  if (m.fast)
+    thread_round<MAXR, TAU, SCORE, kPkPacked>(m, xcol, slot, bs, bs, ra,
+                                              traj_id, st, integ, cnt, o,
+                                              0x7fffffff, 0x7fffffff, false);
+  else
+    thread_round<MAXR, TAU, SCORE, kPkLists>(m, xcol, slot, bs, bs, ra,
+                                             traj_id, st, integ, cnt, o,
+                                             0x7fffffff, 0x7fffffff, false);
   thread_finish<MAXR, SCORE>(m, xcol, bs, st, integ, cnt, o);
 }
 
@@ -945,9 +957,10 @@ __device__ __forceinline__ void any_round(
     thread_round_big<TAU>(m, xcol, slot, bs, ss, ra, traj_id, st, o, cap_ssa,
                           cap_leap, stop_on_switch);
   } else {
-    thread_round<MAXR, TAU, SCORE>(m, xcol, slot, bs, ss, ra, traj_id, st,
-                                   integ, cnt, o, cap_ssa, cap_leap,
-                                   stop_on_switch);
+    thread_round<MAXR, TAU, SCORE, kPkRuntime>(m, xcol, slot, bs, ss, ra,
+                                               traj_id, st, integ, cnt, o,
+                                               cap_ssa, cap_leap,
+                                               stop_on_switch);
   }
 }
 
