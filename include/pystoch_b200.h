@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define PYST_ABI_VERSION 1
+#define PYST_ABI_VERSION 2
 
 /* ---- return codes ------------------------------------------------------ */
 enum {
@@ -53,7 +53,9 @@ enum {
   PYST_TRAJ_OVERFLOW = 3,     /* a species count would leave int32 range   */
   PYST_TRAJ_LEAP_RETRY = 4,   /* tau halved max_leap_retries times         */
   PYST_TRAJ_SAMPLER = 5,      /* Poisson sampler hit its iteration limit   */
-  PYST_TRAJ_STAGING = 6       /* model staging into shared memory timed out */
+  PYST_TRAJ_STAGING = 6,      /* model staging into shared memory timed out */
+  PYST_TRAJ_RATE = 7          /* a kinetic law gave a negative, infinite or
+                                 NaN propensity                            */
 };
 
 /* ---- methods and mappings ---------------------------------------------- */
@@ -74,13 +76,23 @@ enum { PYST_FLAG_UNSORTED = 1 };
 #define PYST_MAX_BLOB_WORDS 12288     /* model blob staged in 48 KiB smem   */
 
 /*
- * Mass-action model description (host pointers).  Matrices are dense,
- * row-major [species][reaction], the layout of SPN.Pre / SPN.Post
+ * Model description (host pointers).  Matrices are dense, row-major
+ * [species][reaction], the layout of SPN.Pre / SPN.Post
  * (mod/petri_net/SPN.py:72-97).
  *
- * Propensity of reaction j:
+ * Propensity of reaction j, mass-action form:
  *   a_j(x) = rate[j] * prod_i prod_{m < order[i][j]} (x_i - m * falling[i][j])
  * computed in FP32 in species order, factors in m order.
+ *
+ * General kinetic laws (the reference pastes any hazard as C source,
+ * mod/parser/parser.py:32-55): reaction j with law_ptr[j+1] > law_ptr[j]
+ * evaluates the postfix program law_code[law_ptr[j] .. law_ptr[j+1]) in FP64
+ * and rounds the result to FP32 (its order column and rate are unused).
+ * Program words are op << 24 | arg:
+ *   1 X i (push x_i)   2 C k (push law_const[k])   3 ADD  4 SUB  5 MUL
+ *   6 DIV   7 IDIV (C integer division: truncate toward zero)   8 NEG
+ *   10 EXP  11 LN  12 SQRT  13 ABS  14 FLOOR  15 CEIL  16 DUP
+ * at most 8 values deep.  law_ptr == NULL: every reaction is mass action.
  */
 typedef struct pyst_model_desc {
   int32_t n_species;           /* S = TlArgs.N                              */
@@ -100,6 +112,10 @@ typedef struct pyst_model_desc {
   double t_max;                /* TlArgs.t_max                              */
   float eta;                   /* TlArgs.eta (0.03)                         */
   int32_t n_c;                 /* TlArgs.n_c (10)                           */
+  const int32_t* law_ptr;      /* [R+1] program ranges, or NULL              */
+  const uint32_t* law_code;    /* [law_ptr[R]] program words                 */
+  const double* law_const;     /* [n_law_const]                              */
+  int32_t n_law_const;
 } pyst_model_desc;
 
 /* Run description.  Trajectory u (0 <= u < n_traj) draws from the Philox
@@ -293,6 +309,10 @@ enum {
   PYST_H_FLAGS = 25,
   PYST_H_TMAX_LO = 26,      /* f64 bits                                     */
   PYST_H_TMAX_HI = 27,
+  PYST_H_OFF_LAWPTR = 28,   /* i32[R+1] kinetic-law program ranges          */
+  PYST_H_OFF_LAW = 29,      /* program words                                */
+  PYST_H_OFF_LAWC = 30,     /* f64[] constants (even word offset)           */
+  PYST_H_NLAW = 31,         /* reactions with a program (0: none)           */
   PYST_H_WORDS_HEADER = 32
 };
 #define PYST_BLOB_MAGIC 0x31545950u

@@ -66,7 +66,9 @@ class _OModel(C.Structure):
                 ('net', C.c_void_p), ('rate', C.c_void_p),
                 ('x0', C.c_void_p), ('hor', C.c_void_p),
                 ('hor_type', C.c_void_p), ('times', C.c_void_p),
-                ('out', C.c_void_p), ('eta', C.c_float), ('n_c', C.c_int)]
+                ('out', C.c_void_p), ('eta', C.c_float), ('n_c', C.c_int),
+                ('law_ptr', C.c_void_p), ('law_code', C.c_void_p),
+                ('law_const', C.c_void_p)]
 
 
 class _ORun(C.Structure):
@@ -200,6 +202,13 @@ def simulate(model, n_traj, method, seed=0, traj_id_base=0, warp=False,
                  arr(model.sample_times, np.float32),
                  arr(model.out_species, np.int32), float(model.eta),
                  int(model.n_c))
+    if getattr(model, 'laws', None) is not None:
+        ptr, code, consts = model.law_arrays()
+        om.law_ptr = arr(ptr, np.int32)
+        om.law_code = arr(code if code.size else np.zeros(1, np.uint32),
+                          np.uint32)
+        om.law_const = arr(consts if consts.size else np.zeros(1),
+                           np.float64)
     ru = _ORun(int(seed), int(traj_id_base), int(method), 1 if warp else 0,
                int(ssa_fallback_steps), int(max_leap_retries),
                int(step_budget))

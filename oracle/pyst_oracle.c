@@ -265,6 +265,10 @@ typedef struct {
   const int32_t* out;       /* [kappa] */
   float eta;
   int n_c;
+  /* general kinetic laws (kinetic.py; engine eval_law): NULL = none */
+  const int32_t* law_ptr;   /* [R+1] */
+  const uint32_t* law_code;
+  const double* law_const;
 } omodel;
 
 typedef struct {
@@ -292,10 +296,80 @@ typedef struct {
 #define FNV_PRIME 0x100000001b3ull
 static uint64_t mix(uint64_t h, uint64_t v) { return (h ^ v) * FNV_PRIME; }
 
-/* Propensity of reaction j: FP32 product, species ascending, factor
- * index ascending. */
+/* Kinetic-law programs (py_stoch_b200/kinetic.py), evaluated in FP64 one
+ * rounded operation at a time like the engine's eval_law
+ * (py_stoch_b200/csrc/pyst_engine.cuh). */
+static double law_idiv(double a, double b) {
+  if (b == 0.0) return NAN;
+  double q = trunc(a / b);
+  double rem = fma(-q, b, a);
+  if (q != 0.0 && rem != 0.0 && ((rem < 0.0) != (a < 0.0)))
+    q = q - copysign(1.0, q);
+  return q;
+}
+
+static double law_exp(double a) {
+  if (!(a == a)) return a;
+  if (a > 709.0) return INFINITY;
+  if (a < -708.0) return 0.0;
+  return oracle_exp(a);
+}
+
+static double law_ln(double a) {
+  if (!(a >= 0.0)) return NAN;
+  if (a == 0.0) return -INFINITY;
+  if (a > 1.7976931348623157e308) return a;
+  return oracle_log(a);
+}
+
+static float eval_law(const omodel* m, int j, const int32_t* x) {
+  double st[8];
+  int sp = 0;
+  for (int c = m->law_ptr[j]; c < m->law_ptr[j + 1]; ++c) {
+    uint32_t wd = m->law_code[c];
+    int op = (int)(wd >> 24), arg = (int)(wd & 0xFFFFFFu);
+    if (op == 1 || op == 2 || op == 16) {
+      if (sp >= 8 || (op == 16 && sp < 1)) return NAN;
+      st[sp] = op == 1 ? (double)x[arg]
+                       : (op == 2 ? m->law_const[arg] : st[sp - 1]);
+      ++sp;
+    } else if (op >= 3 && op <= 7) {
+      if (sp < 2) return NAN;
+      double b = st[--sp], a = st[sp - 1], r;
+      if (op == 3) r = a + b;
+      else if (op == 4) r = a - b;
+      else if (op == 5) r = a * b;
+      else if (op == 6) r = a / b;
+      else r = law_idiv(a, b);
+      st[sp - 1] = r;
+    } else {
+      if (sp < 1) return NAN;
+      double a = st[sp - 1], r;
+      if (op == 8) r = -a;
+      else if (op == 10) r = law_exp(a);
+      else if (op == 11) r = law_ln(a);
+      else if (op == 12) r = sqrt(a);
+      else if (op == 13) r = fabs(a);
+      else if (op == 14) r = floor(a);
+      else if (op == 15) r = ceil(a);
+      else return NAN;
+      st[sp - 1] = r;
+    }
+  }
+  return sp == 1 ? (float)st[0] : NAN;
+}
+
+static int has_law(const omodel* m, int j) {
+  return m->law_ptr && m->law_ptr[j + 1] > m->law_ptr[j];
+}
+
+static int valid_rate(float a) { return a >= 0.0f && a <= 3.4028234663852886e38f; }
+
+/* Propensity of reaction j: the reaction's kinetic-law program, or the
+ * FP32 product, species ascending, factor index ascending. */
 static float prop(const omodel* m, const float* rate32, int j,
                   const int32_t* x) {
+  if (has_law(m, j)) return eval_law(m, j, x);
   float a = rate32[j];
   for (int i = 0; i < m->S; ++i) {
     int n = m->order[(size_t)i * m->R + j];
@@ -437,7 +511,15 @@ static void one_trajectory(const omodel* m, const float* rate32,
   uint32_t leap_q = 0;
 
   for (;;) {
-    for (int j = 0; j < R; ++j) a[j] = prop(m, rate32, j, x);
+    int bad_rate = 0;
+    for (int j = 0; j < R; ++j) {
+      a[j] = prop(m, rate32, j, x);
+      if (m->law_ptr && !valid_rate(a[j])) bad_rate = 1;
+    }
+    if (bad_rate) {
+      status = 7;
+      break;
+    }
     double a0 = total(ru, R, a, NULL, part, incl);
     if (a0 == 0.0) {
       status = 1;

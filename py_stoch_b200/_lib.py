@@ -28,6 +28,7 @@ TRAJ_OVERFLOW = 3
 TRAJ_LEAP_RETRY = 4
 TRAJ_SAMPLER = 5
 TRAJ_STAGING = 6
+TRAJ_RATE = 7
 
 METHOD_DIRECT = 0
 METHOD_TAU_LEAP = 1
@@ -57,7 +58,9 @@ class ModelDesc(C.Structure):
                 ('hor_type', _p), ('sample_times', _p),
                 ('n_samples', C.c_int32), ('out_species', _p),
                 ('n_out', C.c_int32), ('t_max', C.c_double),
-                ('eta', C.c_float), ('n_c', C.c_int32)]
+                ('eta', C.c_float), ('n_c', C.c_int32),
+                ('law_ptr', _p), ('law_code', _p), ('law_const', _p),
+                ('n_law_const', C.c_int32)]
 
 
 class RunDesc(C.Structure):

@@ -59,6 +59,10 @@ class Batch(object):
         self.device = torch.device(device or 'cuda')
         self.models = list(models)
         n = len(self.models)
+        if (score or jacobian) and any(getattr(m, 'has_laws', False)
+                                       for m in self.models):
+            raise ValueError('likelihood-ratio scores need mass-action laws; '
+                             'a model of the batch has general kinetic laws')
         self.n_traj = (np.full(n, int(n_traj), np.int64)
                        if np.isscalar(n_traj) else
                        np.asarray(n_traj, np.int64))

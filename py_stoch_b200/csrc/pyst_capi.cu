@@ -51,6 +51,7 @@ int read_header(const uint32_t* h, HostModelInfo* mi) {
   mi->words = (int)h[PYST_H_WORDS];
   mi->S = (int)h[PYST_H_S];
   mi->R = (int)h[PYST_H_R];
+  mi->nlaw = (int)h[PYST_H_NLAW];
   if (mi->words <= 0 || (mi->words & 3) || mi->words > PYST_MAX_BLOB_WORDS)
     return PYST_EUNSUPPORTED;
   if (mi->S < 1 || mi->R < 1 || mi->S > PYST_MAX_SPECIES ||
@@ -138,7 +139,9 @@ int single_run(const uint32_t* h_blob, const uint32_t* d_blob,
   const uint64_t idb = (uint64_t)run->traj_id_base;
   const int64_t n = run->n_traj;
   if (mapping == PYST_MAP_THREAD && tau &&
-      !(run->flags & PYST_FLAG_UNSORTED)) {
+      !(run->flags & PYST_FLAG_UNSORTED) && mi.nlaw == 0) {
+    // (models with general kinetic laws take the simple tau loop: the
+    // sorted kernel's engine carries no law evaluator)
     const int rc =
         score ? launch_tau_sorted_1(mi.R, d_blob, mi, n, idb, ra, ob, queue,
                                     kSortedCapSsa, kSortedCapLeap, st)
@@ -197,6 +200,7 @@ const char* pyst_traj_status_string(int code) {
     case PYST_TRAJ_LEAP_RETRY: return "tau halved too many times";
     case PYST_TRAJ_SAMPLER: return "Poisson sampler iteration limit";
     case PYST_TRAJ_STAGING: return "model staging timed out";
+    case PYST_TRAJ_RATE: return "kinetic law gave an invalid propensity";
   }
   return "unknown trajectory status";
 }

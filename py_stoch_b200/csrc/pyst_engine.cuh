@@ -105,15 +105,98 @@ __device__ __forceinline__ PoissonKey leap_key(const Stream& s, uint32_t q,
   return pk;
 }
 
-// Propensity of reaction j in FP32 (rate, then factors in entry order).
-template <class XGet>
+// C integer division of two integral FP64 values: the quotient truncated
+// toward zero (exact for |a|, |b| < 2^53: a quotient rounded up onto an
+// integer is stepped back by the sign of the exact remainder).
+__device__ __forceinline__ double law_idiv(double a, double b) {
+  if (b == 0.0) return __longlong_as_double(0x7ff8000000000000ll);
+  double q = trunc(__ddiv_rn(a, b));
+  const double rem = __fma_rn(-q, b, a);
+  if (q != 0.0 && rem != 0.0 && ((rem < 0.0) != (a < 0.0)))
+    q = __dsub_rn(q, copysign(1.0, q));
+  return q;
+}
+
+__device__ __forceinline__ double law_exp(double a) {
+  if (!(a == a)) return a;
+  if (a > 709.0) return __longlong_as_double(0x7ff0000000000000ll);
+  if (a < -708.0) return 0.0;
+  return pyst_exp(a);
+}
+
+__device__ __forceinline__ double law_ln(double a) {
+  if (!(a >= 0.0)) return __longlong_as_double(0x7ff8000000000000ll);
+  if (a == 0.0) return __longlong_as_double((long long)0xfff0000000000000ull);
+  if (a > 1.7976931348623157e308) return a;
+  return pyst_log(a);
+}
+
+// General kinetic law of reaction j (pyst_model_desc: postfix program over
+// the species counts x[i * xs] and FP64 constants), each operation
+// explicitly rounded, the result rounded once to the FP32 propensity.  The
+// packer checks the programs' stacks; a malformed one gives NaN here (and
+// the trajectory the PYST_TRAJ_RATE status).  Out of line: one copy serves
+// every call site.
+static __device__ __noinline__ float eval_law(const ModelView& m, int j,
+                                              const int32_t* x, int xs) {
+  const double nan = __longlong_as_double(0x7ff8000000000000ll);
+  double st[8];
+  int sp = 0;
+  const int c1 = m.lawptr(j + 1);
+  for (int c = m.lawptr(j); c < c1; ++c) {
+    const uint32_t wd = m.law(c);
+    const int op = (int)(wd >> 24), arg = (int)(wd & 0xFFFFFFu);
+    if (op == 1 || op == 2 || op == 16) {
+      if (sp >= 8 || (op == 16 && sp < 1)) return (float)nan;
+      st[sp] = op == 1 ? (double)x[(int64_t)arg * xs]
+                       : (op == 2 ? m.lawc(arg) : st[sp - 1]);
+      ++sp;
+    } else if (op >= 3 && op <= 7) {
+      if (sp < 2) return (float)nan;
+      const double b = st[--sp], a = st[sp - 1];
+      double r;
+      if (op == 3) r = __dadd_rn(a, b);
+      else if (op == 4) r = __dsub_rn(a, b);
+      else if (op == 5) r = __dmul_rn(a, b);
+      else if (op == 6) r = __ddiv_rn(a, b);
+      else r = law_idiv(a, b);
+      st[sp - 1] = r;
+    } else {
+      if (sp < 1) return (float)nan;
+      const double a = st[sp - 1];
+      double r;
+      if (op == 8) r = -a;
+      else if (op == 10) r = law_exp(a);
+      else if (op == 11) r = law_ln(a);
+      else if (op == 12) r = __dsqrt_rn(a);
+      else if (op == 13) r = fabs(a);
+      else if (op == 14) r = floor(a);
+      else if (op == 15) r = ceil(a);
+      else return (float)nan;
+      st[sp - 1] = r;
+    }
+  }
+  return sp == 1 ? __double2float_rn(st[0]) : (float)nan;
+}
+
+// A propensity a kinetic law may return: finite and non-negative.
+__device__ __forceinline__ bool valid_rate(float a) {
+  return a >= 0.0f && a <= 3.4028234663852886e38f;
+}
+
+// Propensity of reaction j in FP32: the reaction's kinetic-law program if
+// it has one (LAWS: the caller supports them), else the rate, then factors
+// in entry order.  Species counts are x[i * xs].
+template <bool LAWS = true>
 __device__ __forceinline__ float propensity(const ModelView& m, int j,
-                                            XGet xget) {
+                                            const int32_t* xc, int xs) {
+  if (LAWS && m.nlaw && m.lawptr(j + 1) > m.lawptr(j))
+    return eval_law(m, j, xc, xs);
   float a = m.rate(j);
   const int e1 = m.facptr(j + 1);
   for (int e = m.facptr(j); e < e1; ++e) {
     const uint32_t fe = m.fac(e);
-    const int x = xget(ent_lo(fe));
+    const int x = xc[(int64_t)ent_lo(fe) * xs];
     const int n = fac_order(fe);
     const int fall = fac_falling(fe);
     for (int q = 0; q < n; ++q) a = __fmul_rn(a, (float)(x - q * fall));
@@ -137,7 +220,7 @@ __device__ __forceinline__ float propensity(const ModelView& m, int j,
 // All threads of the block call this; true when every reaction fits.
 __device__ __forceinline__ bool pack_reactions(const ModelView& m,
                                                uint32_t* pk) {
-  bool ok = true;
+  bool ok = m.nlaw == 0;  // kinetic-law programs use the general path
   for (int j = threadIdx.x; j < m.R; j += blockDim.x) {
     const int e0 = m.facptr(j), e1 = m.facptr(j + 1);
     uint32_t d = 0;
@@ -251,8 +334,9 @@ __device__ __forceinline__ void thread_init(const ModelView& m, int32_t* xcol,
 // scratch of species i is slot[i*ss].  It stops only between steps, so the trajectory resumes
 // exactly where it left off.  With unbounded caps this is the whole
 // trajectory.
-// PK: how reactions are read -- kPkLists (entry lists), kPkPacked (packed
-// descriptors, m.fast must hold) or kPkRuntime (whichever m.fast says).
+// PK: how reactions are read -- kPkLists (entry lists, general kinetic
+// laws included), kPkPacked (packed descriptors, m.fast must hold) or
+// kPkRuntime (whichever m.fast says; mass-action models only).
 // The fixed forms carry only their own code and live registers (faster for
 // the plain kernels); the mode-sorted kernel measured faster with one
 // run-time form.
@@ -265,6 +349,9 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
                              int cap_leap, bool stop_on_switch) {
   const int S = m.S, R = m.R, ita = m.ita, kappa = m.kappa;
   const bool pk = PK == kPkPacked || (PK == kPkRuntime && m.fast);
+  // general kinetic laws: entry-list form only (a model with laws never
+  // packs, and the sorted kernel's run-time form is not given such models)
+  constexpr bool kLaws = PK == kPkLists;
 #define XV(i) xcol[(int64_t)(i) * bs]
 #define SL(i) slot[(int64_t)(i) * ss]
   Stream rs = make_stream(ra.seed, traj_id);
@@ -299,8 +386,21 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
     for (int j = 0; j < MAXR; ++j) {
       if (j >= R) break;
       a[j] = pk ? propensity_packed(m.rate(j), m.pk[j], xget)
-                    : propensity(m, j, xget);
+                    : propensity<kLaws>(m, j, xcol, bs);
       a0 = __dadd_rn(a0, (double)a[j]);
+    }
+    if (kLaws && m.nlaw) {
+      bool bad = false;
+#pragma unroll
+      for (int j = 0; j < MAXR; ++j) {
+        if (j >= R) break;
+        bad |= !valid_rate(a[j]);
+      }
+      if (bad) {
+        status = PYST_TRAJ_RATE;
+        done = true;
+        break;
+      }
     }
     if (a0 == 0.0) {
       status = PYST_TRAJ_ABSORBED;
@@ -718,8 +818,17 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
   while (true) {
     if (n_ssa >= cap_ssa || n_leap >= cap_leap) break;
     double a0 = 0.0;
-    for (int j = 0; j < R; ++j)
-      a0 = __dadd_rn(a0, (double)propensity(m, j, xget));
+    bool bad_rate = false;
+    for (int j = 0; j < R; ++j) {
+      const float aj = propensity(m, j, xcol, bs);
+      bad_rate |= !valid_rate(aj);
+      a0 = __dadd_rn(a0, (double)aj);
+    }
+    if (m.nlaw && bad_rate) {
+      status = PYST_TRAJ_RATE;
+      done = true;
+      break;
+    }
     if (a0 == 0.0) {
       status = PYST_TRAJ_ABSORBED;
       fill_state = true;
@@ -735,7 +844,7 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
       for (int i = 0; i < S; ++i) SL(i) = 0;
       for (int j = 0; j < R; ++j) {
         if (is_critical(m, j, xcol, bs)) continue;
-        const float aj = propensity(m, j, xget);
+        const float aj = propensity(m, j, xcol, bs);
         const int e1 = m.netptr(j + 1);
         for (int e = m.netptr(j); e < e1; ++e) {
           const uint32_t ne = m.net(e);
@@ -768,7 +877,7 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
         double a0c = 0.0;
         for (int j = 0; j < R; ++j)
           if (is_critical(m, j, xcol, bs))
-            a0c = __dadd_rn(a0c, (double)propensity(m, j, xget));
+            a0c = __dadd_rn(a0c, (double)propensity(m, j, xcol, bs));
         double tau2 = __longlong_as_double(0x7ff0000000000000ll);
         uint4 wc = make_uint4(0, 0, 0, 0);
         if (a0c > 0.0) {
@@ -784,7 +893,7 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
           int lastnz = -1;
           for (int j = 0; j < R; ++j) {
             if (!is_critical(m, j, xcol, bs)) continue;
-            const float aj = propensity(m, j, xget);
+            const float aj = propensity(m, j, xcol, bs);
             cum = __dadd_rn(cum, (double)aj);
             if (aj > 0.0f) lastnz = j;
             if (cum >= r) {
@@ -810,7 +919,7 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
               kj = (j == kcrit) ? 1 : 0;
             } else {
               const float lam =
-                  __fmul_rn(propensity(m, j, xget), (float)tau);
+                  __fmul_rn(propensity(m, j, xcol, bs), (float)tau);
               const int k = poisson(lam, leap_key(rs, leap_q, j, retry));
               if (k < 0) bad = true;
               kj = k < 0 ? 0 : k;
@@ -888,7 +997,7 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
       double cum = 0.0;
       int lastnz = -1;
       for (int j = 0; j < R; ++j) {
-        const float aj = propensity(m, j, xget);
+        const float aj = propensity(m, j, xcol, bs);
         cum = __dadd_rn(cum, (double)aj);
         if (aj > 0.0f) lastnz = j;
         if (cum >= r) {
@@ -1079,14 +1188,20 @@ __device__ void run_warp(const ModelView& m, const WarpSmem& ws,
 
   while (true) {
     double part = 0.0;
+    bool bad_rate = false;
     for (int j = j0; j < j1; ++j) {
-      const float aj = propensity(m, j, xget);
+      const float aj = propensity(m, j, ws.x, 1);
+      bad_rate |= !valid_rate(aj);
       ws.a[j] = aj;
       part = __dadd_rn(part, (double)aj);
     }
     const double incl = warp_incl_scan(part, lane);
     const double a0 = __shfl_sync(0xffffffffu, incl, 31);
     __syncwarp();
+    if (__any_sync(0xffffffffu, m.nlaw && bad_rate)) {
+      status = PYST_TRAJ_RATE;
+      break;
+    }
     if (a0 == 0.0) {
       status = PYST_TRAJ_ABSORBED;
       fill_state = true;

@@ -48,6 +48,7 @@ __device__ __forceinline__ void mark_staging_failure(const OutBase& ob,
 
 struct HostModelInfo {
   int S, R, words;
+  int nlaw;  // reactions with a general kinetic law
 };
 
 constexpr size_t kMaxDynSmem = 227 * 1024;

@@ -19,6 +19,7 @@ struct ModelView {
   int S, R, kappa, ita;
   int o_rate, o_facptr, o_fac, o_netptr, o_net, o_times, o_out, o_x0;
   int o_spvptr, o_spv, o_g, o_critptr, o_crit;
+  int o_lawptr, o_law, o_lawc, nlaw;  // general kinetic laws (nlaw = 0: none)
   int n_c;
   float eta;
   double t_max;
@@ -46,6 +47,10 @@ struct ModelView {
     o_g = (int)w[PYST_H_OFF_G];
     o_critptr = (int)w[PYST_H_OFF_CRITPTR];
     o_crit = (int)w[PYST_H_OFF_CRIT];
+    o_lawptr = (int)w[PYST_H_OFF_LAWPTR];
+    o_law = (int)w[PYST_H_OFF_LAW];
+    o_lawc = (int)w[PYST_H_OFF_LAWC];
+    nlaw = (int)w[PYST_H_NLAW];
     n_c = (int)w[PYST_H_NC];
     eta = __uint_as_float(w[PYST_H_ETA]);
     const uint64_t tb = (uint64_t)w[PYST_H_TMAX_LO] |
@@ -80,6 +85,13 @@ struct ModelView {
   }
   __device__ __forceinline__ uint32_t crit(int e) const {
     return w[o_crit + e];
+  }
+  __device__ __forceinline__ int lawptr(int j) const {
+    return (int)w[o_lawptr + j];
+  }
+  __device__ __forceinline__ uint32_t law(int c) const { return w[o_law + c]; }
+  __device__ __forceinline__ double lawc(int k) const {
+    return reinterpret_cast<const double*>(w + o_lawc)[k];
   }
 };
 

@@ -155,6 +155,60 @@ int pack(const pyst_model_desc* m, Packed* out) {
   w[PYST_H_OFF_CRIT] = here();
   w.insert(w.end(), ent.begin(), ent.end());
 
+  // general kinetic laws: program ranges, words, FP64 constants
+  uint32_t nlaw = 0;
+  if (m->law_ptr) {
+    if (m->law_ptr[0] != 0) return PYST_EINVAL;
+    for (int j = 0; j < R; ++j) {
+      if (m->law_ptr[j + 1] < m->law_ptr[j]) return PYST_EINVAL;
+      if (m->law_ptr[j + 1] > m->law_ptr[j]) ++nlaw;
+    }
+    const int ncode = m->law_ptr[R];
+    if (ncode > 0 && !m->law_code) return PYST_EINVAL;
+    if (m->n_law_const < 0 || (m->n_law_const > 0 && !m->law_const))
+      return PYST_EINVAL;
+    // check every program: known op codes, operands in range, and a
+    // stack that never underflows, never exceeds 8 and ends at 1
+    for (int j = 0; j < R; ++j) {
+      if (m->law_ptr[j + 1] == m->law_ptr[j]) continue;
+      int depth = 0;
+      for (int c = m->law_ptr[j]; c < m->law_ptr[j + 1]; ++c) {
+        const uint32_t op = m->law_code[c] >> 24, arg = m->law_code[c] & 0xFFFFFFu;
+        int pops = 0, pushes = 1;
+        if (op == 1) {
+          if ((int)arg >= S) return PYST_EINVAL;
+        } else if (op == 2) {
+          if ((int)arg >= m->n_law_const) return PYST_EINVAL;
+        } else if (op >= 3 && op <= 7) {
+          pops = 2;
+        } else if (op == 8 || (op >= 10 && op <= 15)) {
+          pops = 1;
+        } else if (op == 16) {
+          pops = 1;
+          pushes = 2;
+        } else {
+          return PYST_EINVAL;
+        }
+        if (depth < pops) return PYST_EINVAL;
+        depth += pushes - pops;
+        if (depth > 8) return PYST_EUNSUPPORTED;
+      }
+      if (depth != 1) return PYST_EINVAL;
+    }
+    w[PYST_H_OFF_LAWPTR] = here();
+    for (int j = 0; j <= R; ++j) w.push_back((uint32_t)m->law_ptr[j]);
+    w[PYST_H_OFF_LAW] = here();
+    for (int c = 0; c < ncode; ++c) w.push_back(m->law_code[c]);
+    if (w.size() & 1) w.push_back(0u);
+    w[PYST_H_OFF_LAWC] = here();
+    for (int k = 0; k < m->n_law_const; ++k) {
+      uint64_t b;
+      memcpy(&b, &m->law_const[k], 8);
+      w.push_back((uint32_t)b);
+      w.push_back((uint32_t)(b >> 32));
+    }
+  }
+
   while (w.size() & 3) w.push_back(0u);
   if (w.size() > (size_t)PYST_MAX_BLOB_WORDS) return PYST_EUNSUPPORTED;
 
@@ -167,6 +221,7 @@ int pack(const pyst_model_desc* m, Packed* out) {
   w[PYST_H_NC] = (uint32_t)m->n_c;
   w[PYST_H_ETA] = f32_bits(m->eta);
   w[PYST_H_FLAGS] = 0;
+  w[PYST_H_NLAW] = nlaw;
   uint64_t tb;
   memcpy(&tb, &m->t_max, 8);
   w[PYST_H_TMAX_LO] = (uint32_t)tb;

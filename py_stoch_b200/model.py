@@ -89,16 +89,19 @@ def _eval_rate(ratio, c):
 
 
 class Model(object):
-    """Dense mass-action model (the fields of ``pyst_model_desc``).
+    """Dense model (the fields of ``pyst_model_desc``).
 
     Arrays: order/falling/pre/net [S, R]; rate [R] (float64, rounded to
     FP32 by the packer); x0, hor, hor_type [S]; sample_times [ita] float32;
-    out_species [kappa].
+    out_species [kappa].  ``laws``: None, or per reaction None (mass action)
+    or the (code, constants) program of a general kinetic law
+    (:func:`py_stoch_b200.kinetic.compile_law`); a reaction with a law
+    ignores its order column and rate.
     """
 
     def __init__(self, order, pre, net, rate, x0, sample_times, out_species,
                  hor=None, hor_type=None, falling=None, t_max=None, eta=0.03,
-                 n_c=10, name=''):
+                 n_c=10, name='', laws=None):
         self.order = np.ascontiguousarray(order, dtype=np.int32)
         S, R = self.order.shape
         self.pre = np.ascontiguousarray(pre, dtype=np.int32).reshape(S, R)
@@ -111,8 +114,16 @@ class Model(object):
                                                  dtype=np.float32).ravel()
         self.out_species = np.ascontiguousarray(out_species,
                                                 dtype=np.int32).ravel()
+        self.laws = None
+        if laws is not None and any(l is not None for l in laws):
+            if len(laws) != R:
+                raise ValueError('laws must have one entry per reaction')
+            self.laws = list(laws)
         if hor is None or hor_type is None:
-            hor, hor_type = derive_hors(self.pre, self.order)
+            order_h = self.order.copy()
+            for j in self.law_reactions():
+                order_h[:, j] = self.pre[:, j]
+            hor, hor_type = derive_hors(self.pre, order_h)
         self.hor = np.ascontiguousarray(hor, dtype=np.int32).reshape(S)
         self.hor_type = np.ascontiguousarray(hor_type,
                                              dtype=np.int32).reshape(S)
@@ -122,6 +133,16 @@ class Model(object):
         self.n_c = int(n_c)
         self.name = name
         self._blob = None
+
+    def law_reactions(self):
+        """Indices of the reactions with a general kinetic law."""
+        if self.laws is None:
+            return []
+        return [j for j, l in enumerate(self.laws) if l is not None]
+
+    @property
+    def has_laws(self):
+        return self.laws is not None
 
     @property
     def n_species(self):
@@ -153,12 +174,30 @@ class Model(object):
         order = np.zeros((S, R), np.int32)
         falling = np.ones((S, R), np.uint8)
         rate = np.zeros(R, np.float64)
+        laws = [None] * R
+        from .kinetic import has_int_division
+        n_par = len(np.ravel(args.c))
         for j, hz in enumerate(args.hazard_exprs):
-            o, fl, ratio = analyse_hazard(hz, tuple(int(v) for v in pre[:, j]),
-                                          S)
+            try:
+                if has_int_division(hz, S, n_par):
+                    raise UnsupportedKineticLaw('integer division')
+                o, fl, ratio = analyse_hazard(
+                    hz, tuple(int(v) for v in pre[:, j]), S)
+                r = _eval_rate(ratio, args.c)
+            except UnsupportedKineticLaw:
+                # not k * prod(x_i falling or power): compile the law as
+                # the reference would evaluate it (C typing, FP64)
+                from .kinetic import compile_law, KineticLawError
+                try:
+                    code, consts, _ = compile_law(
+                        hz, S, [float(v) for v in np.ravel(args.c)])
+                except KineticLawError as e:
+                    raise UnsupportedKineticLaw(str(e))
+                laws[j] = (code, consts)
+                continue
             order[:, j] = o
             falling[:, j] = fl
-            rate[j] = _eval_rate(ratio, args.c)
+            rate[j] = r
         hor = getattr(args, 'H', None)
         hor_type = getattr(args, 'H_type', None)
         if hor is None or len(hor) != S:
@@ -166,7 +205,7 @@ class Model(object):
         return cls(order, pre, post - pre, rate, args.x_0, args.I, args.E,
                    hor=hor, hor_type=hor_type, falling=falling,
                    t_max=args.t_max, eta=getattr(args, 'eta', 0.03),
-                   n_c=getattr(args, 'n_c', 10))
+                   n_c=getattr(args, 'n_c', 10), laws=laws)
 
     @classmethod
     def mass_action(cls, pre, post, k, x0, sample_times, out_species=None,
@@ -210,7 +249,35 @@ class Model(object):
         d.t_max = self.t_max
         d.eta = C.c_float(self.eta).value
         d.n_c = self.n_c
+        if self.laws is not None:
+            ptr, code, consts = self.law_arrays()
+            d.law_ptr = ptr.ctypes.data
+            d.law_code = code.ctypes.data if code.size else None
+            d.law_const = consts.ctypes.data if consts.size else None
+            d.n_law_const = int(consts.size)
         return d
+
+    def law_arrays(self):
+        """(law_ptr int32 [R+1], law_code uint32, law_const float64) of the
+        kinetic-law programs, constants pooled (kept alive on the model)."""
+        if getattr(self, '_law_arrays', None) is None:
+            from .kinetic import OP_C
+            ptr, code, consts = [0], [], []
+            for law in (self.laws or [None] * self.n_reactions):
+                if law is not None:
+                    c, k = law
+                    base = len(consts)
+                    for wd in np.asarray(c, dtype=np.uint32):
+                        wd = int(wd)
+                        if wd >> 24 == OP_C:
+                            wd = (OP_C << 24) | ((wd & 0xFFFFFF) + base)
+                        code.append(wd)
+                    consts.extend(float(v) for v in np.ravel(k))
+                ptr.append(len(code))
+            self._law_arrays = (np.asarray(ptr, dtype=np.int32),
+                                np.asarray(code, dtype=np.uint32),
+                                np.asarray(consts, dtype=np.float64))
+        return self._law_arrays
 
     def blob(self):
         """Packed device blob (np.uint32, length a multiple of 4)."""
@@ -233,7 +300,7 @@ class Model(object):
                   self.sample_times, self.out_species, hor=self.hor,
                   hor_type=self.hor_type, falling=self.falling,
                   t_max=self.t_max, eta=self.eta, n_c=self.n_c,
-                  name=self.name)
+                  name=self.name, laws=self.laws)
         return m
 
     def with_x0(self, x0):
@@ -241,7 +308,7 @@ class Model(object):
                      self.sample_times, self.out_species, hor=self.hor,
                      hor_type=self.hor_type, falling=self.falling,
                      t_max=self.t_max, eta=self.eta, n_c=self.n_c,
-                     name=self.name)
+                     name=self.name, laws=self.laws)
 
 
 def derive_hors(pre, order):

@@ -157,14 +157,23 @@ class TlParser(Parser):
         return args_out
 
     @staticmethod
-    def get_reaction_orders(hazards, species):
+    def get_reaction_orders(hazards, species, pre=None):
         """Total polynomial degree of each hazard in the species symbols
-        (``tl_parser.py:81-95``)."""
+        (``tl_parser.py:81-95``).  The reference raises for a law that is
+        not a polynomial in the species (e.g. Michaelis-Menten); given the
+        Pre matrix, such a reaction's order here is its number of reactant
+        molecules instead."""
         orders = []
         syms = sympy.symbols(list(species.keys()))
-        for hazard in hazards:
+        for j, hazard in enumerate(hazards):
             expr = sympy.expand(hazard.replace('^', '**'))
-            poly = sympy.poly(expr, *syms) if syms else None
+            try:
+                poly = sympy.poly(expr, *syms) if syms else None
+            except sympy.PolynomialError:
+                if pre is None:
+                    raise
+                orders.append(int(numpy.asarray(pre)[:, j].sum()))
+                continue
             orders.append(int(poly.total_degree()) if poly is not None else 0)
         return orders
 
@@ -175,8 +184,8 @@ class TlParser(Parser):
         reactions whose hazard mentions it (``tl_parser.py:98-120``)."""
         hors = numpy.zeros(len(spn.P))
         hors_type = numpy.zeros(len(spn.P))
-        orders = TlParser.get_reaction_orders(spn.h, spn.P)
         pre = numpy.asarray(spn.Pre)
+        orders = TlParser.get_reaction_orders(spn.h, spn.P, pre)
         for reaction, j in spn.T.items():
             for species, i in spn.P.items():
                 hazard = spn.h[j]

@@ -32,7 +32,8 @@ MAPPINGS = {'auto': _lib.MAP_AUTO, 'thread': _lib.MAP_THREAD,
 DEFAULT_STEP_BUDGET = 100_000_000
 
 ERROR_STATUSES = (_lib.TRAJ_STEP_BUDGET, _lib.TRAJ_OVERFLOW,
-                  _lib.TRAJ_LEAP_RETRY, _lib.TRAJ_SAMPLER, _lib.TRAJ_STAGING)
+                  _lib.TRAJ_LEAP_RETRY, _lib.TRAJ_SAMPLER, _lib.TRAJ_STAGING,
+                  _lib.TRAJ_RATE)
 
 
 def _torch():
@@ -88,6 +89,10 @@ def simulate(model, n_traj, method='direct', seed=0, traj_id_base=0,
     block scheduler (identical results).
     """
     torch = _torch()
+    if score and getattr(model, 'has_laws', False):
+        raise ValueError('likelihood-ratio scores need mass-action laws (a_j '
+                         'proportional to its rate constant); this model has '
+                         'general kinetic laws')
     device = torch.device(device or 'cuda')
     L = _lib.lib()
     meth = _method(method)

@@ -35,7 +35,7 @@ def test_exports_every_declared_symbol(built_lib):
 
 
 def test_version_and_strings(built_lib):
-    assert built_lib.pyst_abi_version() == 1
+    assert built_lib.pyst_abi_version() == 2
     for code in range(6):
         assert built_lib.pyst_status_string(code)
     for code in range(7):
