@@ -419,7 +419,12 @@ def main():
                                 timeout=datetime.timedelta(seconds=120))
     dev = torch.device('cuda', local)
     torch.cuda.set_device(dev)
-    _build.build()
+    # one rank (re)builds the library if its sources changed; the others
+    # wait, so no two processes compile into the same build directory
+    if rank == 0:
+        _build.build()
+    if world > 1:
+        dist.barrier()
     m, n, meth = wl['model'], wl['n'], wl['method']
     base = rank * n
     stream = torch.cuda.current_stream(dev)
