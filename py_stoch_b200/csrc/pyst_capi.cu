@@ -32,15 +32,16 @@ namespace {
 
 // Round lengths of the mode-sorted tau-leaping kernel: SSA steps and leaps
 // a trajectory advances between two regroupings of its block.  On the
-// Schlogl workload (262144 trajectories) shorter rounds measured faster:
-// 93 ms a step at 32 / 2, 95 at 64 / 4, 100 at 128 / 8, 107 at 256 / 16,
-// 121 at 256 / 32; resizing leap rounds to match the SSA rounds' measured
-// time was slower (124 ms).
+// Schlogl workload (262144 trajectories, 896-thread blocks) 32 / 3 measured
+// 81.0 ms a step, 24 / 2 81.6, 32 / 2 82.8, 48 / 3 83.0; with 1024-thread
+// blocks longer rounds were slower still (128 / 8 100, 256 / 16 107,
+// 256 / 32 121), and resizing leap rounds to match the SSA rounds'
+// measured time was slower too.
 #ifndef PYST_CAP_SSA
 #define PYST_CAP_SSA 32
 #endif
 #ifndef PYST_CAP_LEAP
-#define PYST_CAP_LEAP 2
+#define PYST_CAP_LEAP 3
 #endif
 constexpr int kSortedCapSsa = PYST_CAP_SSA;
 constexpr int kSortedCapLeap = PYST_CAP_LEAP;
