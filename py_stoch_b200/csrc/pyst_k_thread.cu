@@ -18,8 +18,13 @@ namespace pyst {
 // merged at link time; a per-flavour namespace keeps them apart.
 namespace PYST_CAT(thread_flavour_, PYST_TAU, PYST_SCORE) {
 
+// Blocks of 128 threads per SM the register allocation must allow.
+#ifndef PYST_THREAD_MINB
+#define PYST_THREAD_MINB 1
+#endif
+
 template <int MAXR, bool TAU, bool SCORE>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, PYST_THREAD_MINB)
     k_plain_thread(const uint32_t* __restrict__ gblob, int blob_words,
                    int64_t n_traj, uint64_t id_base, RunArgs ra, OutBase ob,
                    unsigned long long* queue) {
