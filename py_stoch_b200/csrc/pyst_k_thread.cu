@@ -18,9 +18,13 @@ namespace pyst {
 // merged at link time; a per-flavour namespace keeps them apart.
 namespace PYST_CAT(thread_flavour_, PYST_TAU, PYST_SCORE) {
 
-// Blocks of 128 threads per SM the register allocation must allow.
+// Blocks of 128 threads per SM the register allocation must allow: 6
+// (at most 80 registers) measured fastest for the throughput-bound
+// telegraph gradient workload (1M trajectories: 221 ms, against 226 at 5,
+// 230 with no bound) and costs the latency-bound 1024-trajectory
+// Lotka-Volterra run under 1%; 8 (64 registers) spills (339 vs 289 ms).
 #ifndef PYST_THREAD_MINB
-#define PYST_THREAD_MINB 1
+#define PYST_THREAD_MINB 6
 #endif
 
 template <int MAXR, bool TAU, bool SCORE>
