@@ -8,6 +8,14 @@
 // examples/schlogl_sim.py:66-80).  Built once per PYST_SCORE flavour.
 #include "pyst_launch.cuh"
 
+// Blocks of 128 threads per SM the register allocation must allow (unset:
+// no bound).
+#ifdef PYST_BATCH_MINB
+#define PYST_BATCH_BOUNDS __launch_bounds__(128, PYST_BATCH_MINB)
+#else
+#define PYST_BATCH_BOUNDS __launch_bounds__(128)
+#endif
+
 namespace pyst {
 // nvcc gives template functions of an anonymous namespace weak external
 // linkage on the host side, so the flavours built from this file would be
@@ -92,7 +100,7 @@ __device__ void item_epilogue(const ModelView& m, const pyst_batch_item& item,
 }
 
 template <bool SCORE>
-__global__ void __launch_bounds__(128)
+__global__ void PYST_BATCH_BOUNDS
     k_batch(const uint32_t* __restrict__ gblobs,
             const pyst_batch_item* __restrict__ items, int64_t n_items,
             RunArgs ra, OutBase ob, unsigned long long* queue,
