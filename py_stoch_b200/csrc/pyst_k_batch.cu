@@ -8,9 +8,14 @@
 // examples/schlogl_sim.py:66-80).  Built once per PYST_SCORE flavour.
 #include "pyst_launch.cuh"
 
-// Blocks of 128 threads per SM the register allocation must allow (unset:
-// no bound).
-#ifdef PYST_BATCH_MINB
+// Blocks of 128 threads per SM the register allocation must allow: 6 (at
+// most 80 registers) measured 11% faster than no bound on the
+// Schlogl/Lotka-Volterra sweep (2048 models, scores, statistics) and 1.5%
+// slower on synthetic networks of up to 256 reactions; 0 leaves it open.
+#ifndef PYST_BATCH_MINB
+#define PYST_BATCH_MINB 6
+#endif
+#if PYST_BATCH_MINB > 0
 #define PYST_BATCH_BOUNDS __launch_bounds__(128, PYST_BATCH_MINB)
 #else
 #define PYST_BATCH_BOUNDS __launch_bounds__(128)
@@ -104,12 +109,15 @@ __global__ void PYST_BATCH_BOUNDS
     k_batch(const uint32_t* __restrict__ gblobs,
             const pyst_batch_item* __restrict__ items, int64_t n_items,
             RunArgs ra, OutBase ob, unsigned long long* queue,
-            int max_blob_words, int warp_bytes, int dyn_bytes) {
+            int max_blob_words, int warp_bytes, int dyn_bytes, int pk_bytes) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ long long s_item;
   uint32_t* sblob = (uint32_t*)smem;
   uint64_t* bar = (uint64_t*)(smem + (size_t)max_blob_words * 4);
-  unsigned char* dyn = smem + (size_t)max_blob_words * 4 + 16;
+  // packed reaction descriptors of the current item (thread mapping)
+  uint32_t* spk = (uint32_t*)(smem + (size_t)max_blob_words * 4 + 16);
+  unsigned char* dyn =
+      smem + (size_t)max_blob_words * 4 + 16 + (size_t)pk_bytes;
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
     fence_barrier_init();
@@ -135,6 +143,12 @@ __global__ void PYST_BATCH_BOUNDS
     parity ^= 1u;
     ModelView m;
     m.load(sblob);
+    if (item.mapping == PYST_MAP_THREAD &&
+        packed_bytes(m.R) <= (size_t)pk_bytes) {
+      // (uniform over the block: every thread reads the same item)
+      m.pk = spk;
+      m.fast = __syncthreads_and(pack_reactions(m, spk)) != 0;
+    }
     const bool tau = item.method == PYST_METHOD_TAU_LEAP;
     if (item.mapping == PYST_MAP_THREAD) {
       int32_t* xcol = (int32_t*)dyn + threadIdx.x;
@@ -188,7 +202,11 @@ int PYST_CAT(launch_batch_, PYST_SCORE, )(
   const size_t thread_bytes = (size_t)bs * lim->max_species * 12;
   const size_t wbytes = wb * (size_t)(bs / 32);
   const size_t dyn = thread_bytes > wbytes ? thread_bytes : wbytes;
-  const size_t smem = (size_t)lim->max_blob_words * 4 + 16 + dyn;
+  const int maxr_pk = lim->max_reactions < PYST_THREAD_MAX_REACTIONS
+                          ? lim->max_reactions
+                          : PYST_THREAD_MAX_REACTIONS;
+  const size_t pk_bytes = packed_bytes(maxr_pk);
+  const size_t smem = (size_t)lim->max_blob_words * 4 + 16 + pk_bytes + dyn;
   if (smem > kMaxDynSmem) return PYST_EUNSUPPORTED;
   auto kf = k_batch<(bool)PYST_SCORE>;
   const int rc = set_smem(kf, smem);
@@ -203,7 +221,7 @@ int PYST_CAT(launch_batch_, PYST_SCORE, )(
   if (grid > n_items) grid = n_items;
   kf<<<(unsigned)grid, bs, smem, st>>>(d_blobs, d_items, n_items, ra, ob,
                                        queue, lim->max_blob_words, (int)wb,
-                                       (int)dyn);
+                                       (int)dyn, (int)pk_bytes);
   return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
 }
 
