@@ -47,8 +47,8 @@ def workloads():
             # trajectories (profiles/k_tau_sorted_schlogl_229376.md):
             # DRAM read + write per trajectory, and warp instructions per
             # reaction event
-            dram_bytes_per_traj=(708.1e6 + 2424.7e6) / 229376,
-            warp_inst_per_event=42965953892 / 4209068063),
+            dram_bytes_per_traj=(519.8e6 + 1382.3e6) / 229376,
+            warp_inst_per_event=41112782222 / 4209068063),
         'lv_ssa': dict(
             model=networks.lotka_volterra(), n=1024, method='direct',
             desc='plain Gillespie direct method, Lotka-Volterra (k1=10, '
