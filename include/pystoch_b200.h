@@ -67,7 +67,7 @@ enum { PYST_MAP_AUTO = 0, PYST_MAP_THREAD = 1, PYST_MAP_WARP = 2 };
  * default mode-sorted block scheduler (same results, slower). */
 enum { PYST_FLAG_UNSORTED = 1 };
 
-/* Limits of this build. */
+/* Limits of this library. */
 #define PYST_MAX_SPECIES 1024
 #define PYST_MAX_REACTIONS 4096
 #define PYST_THREAD_MAX_REACTIONS 32  /* register-array thread kernels; above
