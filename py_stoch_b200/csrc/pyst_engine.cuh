@@ -340,8 +340,15 @@ __device__ __forceinline__ void thread_init(const ModelView& m, int32_t* xcol,
 // The fixed forms carry only their own code and live registers (faster for
 // the plain kernels); the mode-sorted kernel measured faster with one
 // run-time form.
+// LG > 1 (direct method only): LG adjacent lanes run the same trajectory
+// in lockstep, each on its own species column, and lane g computes the
+// Philox block and exponential variate of every LG-th step (g, g + LG, ...);
+// a step takes its variates from the owning lane by shuffle.  The random
+// numbers, and so the trajectory, are those of LG = 1; only the Philox and
+// log work leaves the per-step dependent chain.  The caller lets one lane
+// of the group write the outputs.
 enum { kPkLists = 0, kPkPacked = 1, kPkRuntime = 2 };
-template <int MAXR, bool TAU, bool SCORE, int PK>
+template <int MAXR, bool TAU, bool SCORE, int PK, int LG = 1>
 __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
                              int bs, int ss, const RunArgs& ra,
                              uint64_t traj_id, TState& st, double* integ,
@@ -359,8 +366,27 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
   // The main stream is stateless, so its next block (and that block's
   // exponential variate) is computed one step ahead, off the dependent
   // chain of the current step; rs.n runs one block ahead of use.
-  uint4 w_pf = next_block(rs);
-  double e_pf = -pyst_log(u53(w_pf.x, w_pf.y));
+  static_assert(LG == 1 || (!TAU && LG <= 16 && (LG & (LG - 1)) == 0),
+                "lane groups: direct method, power of two up to 16 lanes");
+  uint4 w_pf = make_uint4(0u, 0u, 0u, 0u);
+  double e_pf = 0.0;
+  // lane-group variates: block g_base + g_lane, consumed at step g_i
+  const int g_lane = LG > 1 ? (int)(threadIdx.x & (LG - 1)) : 0;
+  const unsigned g_mask =
+      LG > 1 ? ((1u << (LG & 31)) - 1u) << (threadIdx.x & 31 & ~(LG - 1))
+             : 0u;
+  uint64_t g_base = st.n;
+  int g_i = 0;
+  double g_e = 0.0, g_u = 0.0;
+  if constexpr (LG > 1) {
+    rs.n = g_base + (uint64_t)g_lane;
+    const uint4 wg = next_block(rs);
+    g_e = -pyst_log(u53(wg.x, wg.y));
+    g_u = u53(wg.z, wg.w);
+  } else {
+    w_pf = next_block(rs);
+    e_pf = -pyst_log(u53(w_pf.x, w_pf.y));
+  }
   double t = st.t;
   int f = st.f;
   int64_t events = st.events, steps = st.steps;
@@ -622,11 +648,27 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
     // ------------------------ one direct-method step -------------------
     steps++;
     n_ssa++;
-    const uint4 w = w_pf;
-    const double tau = __ddiv_rn(e_pf, a0);
-    w_pf = next_block(rs);
-    e_pf = -pyst_log(u53(w_pf.x, w_pf.y));
-    const double r = __dmul_rn(u53(w.z, w.w), a0);
+    double tau, r;
+    if constexpr (LG > 1) {
+      const double e = __shfl_sync(g_mask, g_e, g_i, LG);
+      const double uu = __shfl_sync(g_mask, g_u, g_i, LG);
+      tau = __ddiv_rn(e, a0);
+      r = __dmul_rn(uu, a0);
+      if (++g_i == LG) {
+        g_i = 0;
+        g_base += LG;
+        rs.n = g_base + (uint64_t)g_lane;
+        const uint4 wg = next_block(rs);
+        g_e = -pyst_log(u53(wg.x, wg.y));
+        g_u = u53(wg.z, wg.w);
+      }
+    } else {
+      const uint4 w = w_pf;
+      tau = __ddiv_rn(e_pf, a0);
+      w_pf = next_block(rs);
+      e_pf = -pyst_log(u53(w_pf.x, w_pf.y));
+      r = __dmul_rn(u53(w.z, w.w), a0);
+    }
     int sel = -1;
     {
       double cum = 0.0;
@@ -655,7 +697,9 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
       }
     }
     while (tn >= tf) {
-      for (int k = 0; k < kappa; ++k) store_sample(o, ita, k, f, XV(m.out(k)));
+      if (LG == 1 || g_lane == 0)
+        for (int k = 0; k < kappa; ++k)
+          store_sample(o, ita, k, f, XV(m.out(k)));
       f++;
       if (f == ita) {
         done = true;
@@ -705,7 +749,8 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
     }
   }
   st.t = t;
-  st.n = rs.n - 1;  // the prefetched block was not used
+  // the prefetched block (LG = 1) was not used
+  st.n = LG > 1 ? g_base + (uint64_t)g_i : rs.n - 1;
   st.events = events;
   st.steps = steps;
   st.h = h;

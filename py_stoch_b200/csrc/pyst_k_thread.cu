@@ -79,6 +79,79 @@ __global__ void __launch_bounds__(128, PYST_THREAD_MINB)
   }
 }
 
+#if !PYST_TAU && !PYST_SCORE
+// Lane groups for runs too small to fill the GPU (direct method): each
+// trajectory is a long dependent chain of steps, so with at most a few
+// warps per SM the step latency, not issue throughput, sets the time.
+// kGroupLanes lanes share one trajectory (thread_round's LG form), which
+// takes the Philox and log work of the other steps off each step's chain.
+// Trajectory u is group u (static assignment); lane 0 of a group writes.
+constexpr int kGroupLanes = 8;
+
+template <int MAXR, int LG>
+__global__ void __launch_bounds__(128)
+    k_plain_group(const uint32_t* __restrict__ gblob, int blob_words,
+                  int64_t n_traj, uint64_t id_base, RunArgs ra, OutBase ob) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint32_t* sblob = (uint32_t*)smem;
+  uint64_t* bar = (uint64_t*)(smem + (size_t)blob_words * 4);
+  const int R = (int)__ldg(gblob + PYST_H_R);
+  uint32_t* pk = (uint32_t*)(smem + (size_t)blob_words * 4 + 16);
+  int32_t* xbase = (int32_t*)((unsigned char*)pk + packed_bytes(R));
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const bool ok = stage_blob(sblob, gblob, blob_words, bar, 0);
+  const int bs = blockDim.x;
+  const int64_t ngroups = (int64_t)gridDim.x * bs / LG;
+  const bool leader = (threadIdx.x & (LG - 1)) == 0;
+  int64_t u = (blockIdx.x * (int64_t)bs + threadIdx.x) / LG;
+  if (!ok) {
+    mbar_wait(bar, 0);  // let a late copy land before the block exits
+    for (; u < n_traj; u += ngroups)
+      if (leader) mark_staging_failure(ob, u);
+    return;
+  }
+  ModelView m;
+  m.load(sblob);
+  m.pk = pk;
+  m.fast = __syncthreads_and(pack_reactions(m, pk)) != 0;
+  int32_t* xcol = xbase + threadIdx.x;
+  int64_t* slot = (int64_t*)(xbase + (size_t)m.S * bs) + threadIdx.x;
+  for (; u < n_traj; u += ngroups) {
+    const TrajOut o = ob.at(0, u, 0, 0, ob.stride, m.R);
+    const uint64_t id = id_base + (uint64_t)u;
+    TState st;
+    thread_init<false>(m, xcol, bs, st);
+    double integ[1] = {0.0};
+    int cnt[1] = {0};
+    if (m.fast)
+      thread_round<MAXR, false, false, kPkPacked, LG>(
+          m, xcol, slot, bs, bs, ra, id, st, integ, cnt, o, 0x7fffffff,
+          0x7fffffff, false);
+    else
+      thread_round<MAXR, false, false, kPkLists, LG>(
+          m, xcol, slot, bs, bs, ra, id, st, integ, cnt, o, 0x7fffffff,
+          0x7fffffff, false);
+    if (leader) thread_finish<MAXR, false>(m, xcol, bs, st, integ, cnt, o);
+  }
+}
+
+template <int MR>
+int launch_group(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
+                 uint64_t id_base, const RunArgs& ra, const OutBase& ob,
+                 int bs, cudaStream_t st, size_t smem) {
+  auto kf = k_plain_group<MR, kGroupLanes>;
+  const int rc = set_smem(kf, smem);
+  if (rc) return rc;
+  const int64_t grid = (n * kGroupLanes + bs - 1) / bs;
+  kf<<<(unsigned)grid, bs, smem, st>>>(d_blob, mi.words, n, id_base, ra, ob);
+  return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
+}
+#endif
+
 template <int MR>
 int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
                uint64_t id_base, const RunArgs& ra, const OutBase& ob, int bs,
@@ -118,6 +191,15 @@ int PYST_CAT(launch_plain_thread_, PYST_TAU, PYST_SCORE)(
     return launch_one<0>(d_blob, mi, n, id_base, ra, ob, bs, st, smem, queue);
 #else
   if (maxr > PYST_THREAD_MAX_REACTIONS) return PYST_EUNSUPPORTED;
+#endif
+#if !PYST_TAU && !PYST_SCORE
+  // fewer trajectories than one 128-thread block of lane groups per SM
+  if (maxr <= 8 && bs <= 128 && bs % kGroupLanes == 0 &&
+      n * kGroupLanes <= (int64_t)num_sms() * 128) {
+    if (maxr <= 4)
+      return launch_group<4>(d_blob, mi, n, id_base, ra, ob, bs, st, smem);
+    return launch_group<8>(d_blob, mi, n, id_base, ra, ob, bs, st, smem);
+  }
 #endif
   if (maxr <= 4)
     return launch_one<4>(d_blob, mi, n, id_base, ra, ob, bs, st, smem, queue);
