@@ -366,15 +366,16 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
   // The main stream is stateless, so its next block (and that block's
   // exponential variate) is computed one step ahead, off the dependent
   // chain of the current step; rs.n runs one block ahead of use.
-  static_assert(LG == 1 || (!TAU && LG <= 16 && (LG & (LG - 1)) == 0),
-                "lane groups: direct method, power of two up to 16 lanes");
+  static_assert(LG == 1 || (!TAU && LG <= 32 && (LG & (LG - 1)) == 0),
+                "lane groups: direct method, power of two up to 32 lanes");
   uint4 w_pf = make_uint4(0u, 0u, 0u, 0u);
   double e_pf = 0.0;
   // lane-group variates: block g_base + g_lane, consumed at step g_i
   const int g_lane = LG > 1 ? (int)(threadIdx.x & (LG - 1)) : 0;
   const unsigned g_mask =
-      LG > 1 ? ((1u << (LG & 31)) - 1u) << (threadIdx.x & 31 & ~(LG - 1))
-             : 0u;
+      LG == 32 ? 0xffffffffu
+      : LG > 1 ? ((1u << (LG & 31)) - 1u) << (threadIdx.x & 31 & ~(LG - 1))
+               : 0u;
   uint64_t g_base = st.n;
   int g_i = 0;
   double g_e = 0.0, g_u = 0.0;

@@ -86,7 +86,15 @@ __global__ void __launch_bounds__(128, PYST_THREAD_MINB)
 // kGroupLanes lanes share one trajectory (thread_round's LG form), which
 // takes the Philox and log work of the other steps off each step's chain.
 // Trajectory u is group u (static assignment); lane 0 of a group writes.
-constexpr int kGroupLanes = 8;
+// A whole warp per trajectory measured fastest (Lotka-Volterra, 1024
+// trajectories: 206.7 ms at 32 lanes, 217.1 at 16, 236.1 at 8): the warp
+// then never diverges between trajectories.
+#ifndef PYST_GROUP_LANES
+#define PYST_GROUP_LANES 32
+#endif
+constexpr int kGroupLanes = PYST_GROUP_LANES;
+// runs of at most this many trajectories per SM take the lane groups
+constexpr int kGroupMaxPerSm = 16;
 
 template <int MAXR, int LG>
 __global__ void __launch_bounds__(128)
@@ -195,7 +203,7 @@ int PYST_CAT(launch_plain_thread_, PYST_TAU, PYST_SCORE)(
 #if !PYST_TAU && !PYST_SCORE
   // fewer trajectories than one 128-thread block of lane groups per SM
   if (maxr <= 8 && bs <= 128 && bs % kGroupLanes == 0 &&
-      n * kGroupLanes <= (int64_t)num_sms() * 128) {
+      n <= (int64_t)num_sms() * kGroupMaxPerSm) {
     if (maxr <= 4)
       return launch_group<4>(d_blob, mi, n, id_base, ra, ob, bs, st, smem);
     return launch_group<8>(d_blob, mi, n, id_base, ra, ob, bs, st, smem);

@@ -140,8 +140,8 @@ def test_schlogl_direct(torch_cuda, built_lib, oracle_mod, mapping):
 @pytest.mark.parametrize('n', [100, 2368, 2369, 4096])
 def test_direct_thread_run_sizes(torch_cuda, built_lib, oracle_mod, n):
     """Direct-method thread runs on both sides of the lane-group limit
-    (8 lanes per trajectory up to 148 x 16 trajectories, one per thread
-    above it, where the runs fill the GPU)."""
+    (a warp per trajectory up to 148 x 16 trajectories, one thread per
+    trajectory above it, where the runs fill the GPU)."""
     m = networks.schlogl(t_end=1.0, n_samples=21)
     g = _gpu(torch_cuda, m, n, 'direct', 'thread', seed=3)
     o = _oracle(oracle_mod, m, n, 'direct', 'thread', seed=3)
