@@ -54,7 +54,11 @@ def workloads():
             desc='plain Gillespie direct method, Lotka-Volterra (k1=10, '
                  'k2=0.01, k3=10), X0=Y0=1000, 1024 trajectories, t_end=10,'
                  ' 100 samples, Philox ids 0..1023',
-            cpu_pilot=64, ref_config='lv_ssa_1024'),
+            cpu_pilot=64, ref_config='lv_ssa_1024',
+            # warp instructions per reaction event of the lane-group
+            # kernel, from one ncu capture of this workload
+            # (profiles/k_plain_group_lv_1024.md)
+            warp_inst_per_event=64533376180 / 307266234),
         'telegraph_grad': dict(
             model=networks.telegraph(), n=1048576, method='direct', grad=True,
             desc='adjoint gradient: telegraph gene expression (k_on=0.5, '
