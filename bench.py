@@ -12,9 +12,13 @@ each leap).  At N GPUs every rank simulates its own 262,144 trajectories
 (distinct Philox ids; weak scaling, no data-path collective) and the value
 is all events over the slowest rank's device time.
 
-One JSON line on rank 0.  ``--impl reference`` times the CPU restatement of
-the reference algorithm (the oracle port; the reference itself is PyCUDA
-code that cannot run here) on all host cores over a bounded sample.
+One JSON line on rank 0.  ``--impl reference`` times the reference's own
+implementation of the path: its CUDA kernels (kernel_P1_P2 / kernel_P3, or
+kernel_Gillespie), compiled for sm_100a from the reference's sources by
+oracle/build_ref.py, driven by a replay of CuTauLeaping.run's host round
+loop (oracle/ref_harness.py).  Where those kernels are not built for the
+workload it falls back to the CPU oracle port on all host cores over a
+bounded sample.
 """
 
 import argparse
@@ -44,9 +48,8 @@ def workloads():
                  'SSA fallback, 262144 trajectories, t_end=5, 200 samples',
             cpu_pilot=1024, ref_config='schlogl_tl_262144',
             # from one ncu capture of the simulation kernel on 229,376
-            # trajectories (profiles/k_tau_sorted_schlogl_229376.md):
-            # DRAM read + write per trajectory, and warp instructions per
-            # reaction event
+            # trajectories: DRAM read + write per trajectory, and warp
+            # instructions per reaction event
             dram_bytes_per_traj=(519.8e6 + 1382.3e6) / 229376,
             warp_inst_per_event=41112782222 / 4209068063),
         'lv_ssa': dict(
@@ -57,7 +60,6 @@ def workloads():
             cpu_pilot=64, ref_config='lv_ssa_1024',
             # warp instructions per reaction event of the lane-group
             # kernel, from one ncu capture of this workload
-            # (profiles/k_plain_group_lv_1024.md)
             warp_inst_per_event=64533376180 / 307266234),
         'telegraph_grad': dict(
             model=networks.telegraph(), n=1048576, method='direct', grad=True,

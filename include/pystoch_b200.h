@@ -54,8 +54,11 @@ enum {
   PYST_TRAJ_LEAP_RETRY = 4,   /* tau halved max_leap_retries times         */
   PYST_TRAJ_SAMPLER = 5,      /* Poisson sampler hit its iteration limit   */
   PYST_TRAJ_STAGING = 6,      /* model staging into shared memory timed out */
-  PYST_TRAJ_RATE = 7          /* a kinetic law gave a negative, infinite or
+  PYST_TRAJ_RATE = 7,         /* a kinetic law gave a negative, infinite or
                                  NaN propensity                            */
+  PYST_TRAJ_UNSUPPORTED = 8   /* batched run with scores: the item's model
+                                 has general kinetic laws, so it was not
+                                 simulated (samples -1, scores NaN)        */
 };
 
 /* ---- methods and mappings ---------------------------------------------- */
@@ -142,7 +145,11 @@ typedef struct pyst_outputs {
   int64_t* events;    /* [n_traj] reaction firings                          */
   uint64_t* seqhash;  /* [n_traj] FNV-1a hash of the firing sequence        */
   double* t_final;    /* [n_traj] clock when the trajectory stopped         */
-  double* score;      /* [n_traj][R] d log p / d log rate_j                 */
+  double* score;      /* [n_traj][R] d log p / d log rate_j; mass-action
+                         models only (the run calls return
+                         PYST_EUNSUPPORTED for a model with general
+                         kinetic laws, batched runs mark such an item's
+                         trajectories PYST_TRAJ_UNSUPPORTED)               */
   double* stats;      /* batched runs: per item [kappa][ita][3] mean,
                          variance, lag-1 correlation with the next sample */
   double* jacobian;   /* batched runs with scores: per item [2][kappa][ita][R]
@@ -250,6 +257,58 @@ int pyst_score_backward(const int32_t* samples, const double* score,
                         const double* gvar, double* d_grad,
                         void* d_workspace, size_t workspace_bytes,
                         void* stream);
+
+/* ---- sufficient statistics for trajectories split across GPUs --------- */
+
+/* The reference's only cross-trajectory reduction is the termination sum
+ * gpuarray.sum(d_Q) (mod/simulator/cuTauLeaping/cuTauLeaping.py:72).  These
+ * four calls extend it to the sample moments and their likelihood-ratio
+ * gradients, in a form that gives the same bits however the trajectories
+ * are split across GPUs (each GPU running a contiguous range of global
+ * Philox ids):
+ *
+ *   pyst_sample_sums        per GPU: exact integer sums over its
+ *                           trajectories, summed across GPUs with an
+ *                           integer all-reduce (order-free, exact);
+ *   pyst_moments_from_sums  every GPU: mean and variance from the totals;
+ *   pyst_score_partials     per GPU: the backward reduction's partial sums,
+ *                           one row of R per PYST_SCORE_CHUNK trajectories;
+ *   pyst_score_combine      every GPU, after gathering all rows in global
+ *                           trajectory order: the gradient.
+ *
+ * With ranges that start on multiples of PYST_SCORE_CHUNK, the moments and
+ * gradient equal those of one GPU running every trajectory (pyst_score_
+ * backward = pyst_score_partials + pyst_score_combine), bit for bit. */
+#define PYST_SCORE_CHUNK 256
+#define PYST_SUMS_MAX_TRAJ 2147483647LL
+
+/* d_sums[kf][3] (int64, kf < kappa*ita) = sum over u < n_traj of x, of
+ * (x*x) >> 32 and of (x*x) & 0xFFFFFFFF, x = samples[kf*stride + u]
+ * (stride 0: n_traj).  Exact for n_traj <= PYST_SUMS_MAX_TRAJ. */
+int pyst_sample_sums(const int32_t* samples, int64_t n_traj, int64_t stride,
+                     int32_t kappa, int32_t ita, int64_t* d_sums,
+                     void* stream);
+
+/* d_mean[kf] = sx / n_total, d_var[kf] = (hi * 2^32 + lo) / n_total -
+ * mean^2 (population variance) from the n_rows rows of d_sums. */
+int pyst_moments_from_sums(const int64_t* d_sums, int32_t n_rows,
+                           int64_t n_total, double* d_mean, double* d_var,
+                           void* stream);
+
+/* d_part[b][j] = sum over trajectories u of chunk b (PYST_SCORE_CHUNK of
+ * them, in order) of h_u * score[u][j], h_u as in pyst_score_backward;
+ * ceil(n_traj / PYST_SCORE_CHUNK) rows of n_reactions doubles. */
+int pyst_score_partials(const int32_t* samples, const double* score,
+                        int64_t n_traj, int32_t kappa, int32_t ita,
+                        int32_t n_reactions, const double* mean,
+                        const double* var, const double* gmean,
+                        const double* gvar, double* d_part, void* stream);
+
+/* d_grad[j] = (sum over the n_blocks rows of d_part, in row order) /
+ * n_total. */
+int pyst_score_combine(const double* d_part, int64_t n_blocks,
+                       int32_t n_reactions, int64_t n_total, double* d_grad,
+                       void* stream);
 
 /* Same reduction as pyst_score_backward, for callers that cannot allocate
  * the workspace themselves: a host runtime that has already handed all

@@ -33,6 +33,14 @@ int pyst_test_math(const double* d_x, int64_t n, int which, double* d_out,
 int pyst_test_poisson(const float* d_lam, int64_t n, uint64_t seed,
                       int32_t* d_out, void* stream);
 
+/* Bound of the model-staging wait of every later run call in this process
+ * (polls of the staging mbarrier; PYST_MBAR_POLL_LIMIT by default).  With
+ * 0 every staging wait gives up at once, so a test can see the timeout
+ * path run: each block then waits, bounded, for its in-flight copy before
+ * moving on, and marks its trajectories PYST_TRAJ_STAGING.  polls < 0
+ * restores the default.  Returns the previous bound. */
+int pyst_test_set_staging_polls(int32_t polls);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,11 +37,17 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 OUT = os.path.join(HERE, '_ref')
+# where this recipe looks for the reference checkout: $PYST_REFERENCE_DIR,
+# else the build container's mount point
 DEFAULT_REF = '/root/reference'
 
 
-def reference_present(ref=DEFAULT_REF):
-    return os.path.isdir(os.path.join(ref, 'mod'))
+def reference_dir():
+    return os.environ.get('PYST_REFERENCE_DIR') or DEFAULT_REF
+
+
+def reference_present(ref=None):
+    return os.path.isdir(os.path.join(ref or reference_dir(), 'mod'))
 
 # name -> (fixture, species_init, params, output species, t_max, ita, U,
 #          gillespie flag, simulator class)
@@ -107,7 +113,8 @@ def _arr(a):
             'shape': list(a.shape)}
 
 
-def build(ref=DEFAULT_REF, names=None):
+def build(ref=None, names=None):
+    ref = ref or reference_dir()
     os.makedirs(OUT, exist_ok=True)
     G = _load_golden_module()
     from py_stoch_b200 import sbml as fake_libsbml
@@ -165,5 +172,5 @@ def build(ref=DEFAULT_REF, names=None):
 
 if __name__ == '__main__':
     sys.path.insert(0, REPO)
-    build(sys.argv[1] if len(sys.argv) > 1 else DEFAULT_REF)
+    build(sys.argv[1] if len(sys.argv) > 1 else reference_dir())
     print('built', OUT)

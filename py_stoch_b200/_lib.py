@@ -10,9 +10,7 @@ import os
 import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-# PYST_LIB selects another build of the library (e.g. an experimental one)
-LIB_PATH = os.environ.get('PYST_LIB') or os.path.join(_HERE,
-                                                       'libpystoch_b200.so')
+LIB_PATH = os.path.join(_HERE, 'libpystoch_b200.so')
 
 PYST_OK = 0
 PYST_EINVAL = 1
@@ -29,6 +27,7 @@ TRAJ_LEAP_RETRY = 4
 TRAJ_SAMPLER = 5
 TRAJ_STAGING = 6
 TRAJ_RATE = 7
+TRAJ_UNSUPPORTED = 8
 
 METHOD_DIRECT = 0
 METHOD_TAU_LEAP = 1
@@ -43,6 +42,8 @@ THREAD_MAX_REACTIONS = 32
 MAX_BLOB_WORDS = 12288
 RUN_WORKSPACE_BYTES = 256
 NOALLOC_SCRATCH_BYTES = 1 << 20
+SCORE_CHUNK = 256
+SUMS_MAX_TRAJ = 2**31 - 1
 
 # header word indices (PYST_H_*)
 H_MAGIC, H_WORDS, H_S, H_R, H_KAPPA, H_ITA = 0, 1, 2, 3, 4, 5
@@ -119,11 +120,21 @@ SIGNATURES = {
     'pyst_score_backward_noalloc': (C.c_int, [_p, _p, C.c_int64, C.c_int32,
                                               C.c_int32, C.c_int32, _p, _p,
                                               _p, _p, _p, _p]),
+    'pyst_sample_sums': (C.c_int, [_p, C.c_int64, C.c_int64, C.c_int32,
+                                   C.c_int32, _p, _p]),
+    'pyst_moments_from_sums': (C.c_int, [_p, C.c_int32, C.c_int64, _p, _p,
+                                         _p]),
+    'pyst_score_partials': (C.c_int, [_p, _p, C.c_int64, C.c_int32,
+                                      C.c_int32, C.c_int32, _p, _p, _p, _p,
+                                      _p, _p]),
+    'pyst_score_combine': (C.c_int, [_p, C.c_int64, C.c_int32, C.c_int64,
+                                     _p, _p]),
     'pyst_test_philox': (C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64,
                                    C.c_int64, _p, _p]),
     'pyst_test_philox_raw': (C.c_int, [_p, C.c_int64, _p, C.c_int, _p]),
     'pyst_test_math': (C.c_int, [_p, C.c_int64, C.c_int, _p, _p]),
     'pyst_test_poisson': (C.c_int, [_p, C.c_int64, C.c_uint64, _p, _p]),
+    'pyst_test_set_staging_polls': (C.c_int, [C.c_int32]),
 }
 
 _lock = threading.Lock()

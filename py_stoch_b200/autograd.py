@@ -31,11 +31,13 @@ from .simulator import _torch, simulate
 
 
 def _moments(samples):
-    torch = _torch()
-    x = samples.to(torch.float64)
-    mean = x.mean(dim=2)
-    var = (x * x).mean(dim=2) - mean * mean
-    return mean.contiguous(), var.contiguous()
+    """Population mean and variance [kappa, ita] of ``samples`` [kappa, ita,
+    U] from exact integer sums on the GPU (the same kernels, and so the same
+    bits, as the multi-GPU reduction in :mod:`py_stoch_b200.shard`)."""
+    from .shard import KernelOps
+    kappa, ita, U = samples.shape
+    ops = KernelOps()
+    return ops.moments(ops.sample_sums(samples), U, kappa, ita)
 
 
 def score_backward(samples, score, mean, var, grad_mean, grad_var,

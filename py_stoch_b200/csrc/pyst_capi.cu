@@ -7,6 +7,7 @@
 
 #include "pyst_launch.cuh"
 #include "pystoch_b200.h"
+#include "pystoch_b200_testing.h"
 
 namespace pyst {
 
@@ -79,8 +80,12 @@ int check_run(const pyst_run_desc* run) {
   return PYST_OK;
 }
 
+// Bound of the model-staging wait (pyst_test_set_staging_polls).
+std::atomic<int> g_stage_polls{PYST_MBAR_POLL_LIMIT};
+
 RunArgs make_args(const pyst_run_desc* run) {
   RunArgs ra;
+  ra.stage_polls = g_stage_polls.load();
   ra.seed = run->seed;
   ra.step_budget = run->step_budget ? run->step_budget : (1ll << 62);
   ra.ssa_fallback_steps =
@@ -119,8 +124,12 @@ int single_run(const uint32_t* h_blob, const uint32_t* d_blob,
     return PYST_EINVAL;
   if (!d_workspace || ((uintptr_t)d_workspace & 7)) return PYST_EINVAL;
   if (workspace_bytes < PYST_RUN_WORKSPACE_BYTES) return PYST_EWORKSPACE;
-  if (run->n_traj == 0) return PYST_OK;
   if (out->stats || out->jacobian) return PYST_EINVAL;  // batched runs only
+  // a likelihood-ratio score N_j - int a_j dt is d log p / d log rate_j only
+  // when a_j is proportional to rate_j (mass action); a general kinetic law
+  // leaves the rate column unused
+  if (out->score && mi.nlaw > 0) return PYST_EUNSUPPORTED;
+  if (run->n_traj == 0) return PYST_OK;
   const RunArgs ra = make_args(run);
   const OutBase ob = make_outbase(out, run->n_traj);
   unsigned long long* queue = (unsigned long long*)d_workspace;
@@ -180,6 +189,10 @@ extern "C" {
 
 int pyst_abi_version(void) { return PYST_ABI_VERSION; }
 
+int pyst_test_set_staging_polls(int32_t polls) {
+  return g_stage_polls.exchange(polls < 0 ? PYST_MBAR_POLL_LIMIT : polls);
+}
+
 const char* pyst_status_string(int code) {
   switch (code) {
     case PYST_OK: return "ok";
@@ -202,6 +215,8 @@ const char* pyst_traj_status_string(int code) {
     case PYST_TRAJ_SAMPLER: return "Poisson sampler iteration limit";
     case PYST_TRAJ_STAGING: return "model staging timed out";
     case PYST_TRAJ_RATE: return "kinetic law gave an invalid propensity";
+    case PYST_TRAJ_UNSUPPORTED:
+      return "scores requested for a model with general kinetic laws";
   }
   return "unknown trajectory status";
 }
@@ -293,6 +308,50 @@ int pyst_score_backward(const int32_t* samples, const double* score,
                                n_reactions, mean, var, gmean, gvar,
                                (double*)d_workspace, d_grad,
                                (cudaStream_t)stream);
+}
+
+int pyst_sample_sums(const int32_t* samples, int64_t n_traj, int64_t stride,
+                     int32_t kappa, int32_t ita, int64_t* d_sums,
+                     void* stream) {
+  if (!samples || !d_sums || n_traj < 0 || n_traj > PYST_SUMS_MAX_TRAJ ||
+      kappa < 1 || ita < 1)
+    return PYST_EINVAL;
+  if (stride == 0) stride = n_traj;
+  if (stride < n_traj) return PYST_EINVAL;
+  return launch_sample_sums(samples, n_traj, stride, kappa * ita, d_sums,
+                            (cudaStream_t)stream);
+}
+
+int pyst_moments_from_sums(const int64_t* d_sums, int32_t n_rows,
+                           int64_t n_total, double* d_mean, double* d_var,
+                           void* stream) {
+  if (!d_sums || !d_mean || !d_var || n_rows < 1 || n_total < 1)
+    return PYST_EINVAL;
+  return launch_moments_from_sums(d_sums, n_rows, n_total, d_mean, d_var,
+                                  (cudaStream_t)stream);
+}
+
+int pyst_score_partials(const int32_t* samples, const double* score,
+                        int64_t n_traj, int32_t kappa, int32_t ita,
+                        int32_t n_reactions, const double* mean,
+                        const double* var, const double* gmean,
+                        const double* gvar, double* d_part, void* stream) {
+  if (!samples || !score || !mean || !gmean || !d_part || n_traj < 1 ||
+      kappa < 1 || ita < 1 || n_reactions < 1)
+    return PYST_EINVAL;
+  if (gvar && !var) return PYST_EINVAL;
+  return launch_score_partials(samples, score, n_traj, kappa, ita,
+                               n_reactions, mean, var, gmean, gvar, d_part,
+                               (cudaStream_t)stream);
+}
+
+int pyst_score_combine(const double* d_part, int64_t n_blocks,
+                       int32_t n_reactions, int64_t n_total, double* d_grad,
+                       void* stream) {
+  if (!d_part || !d_grad || n_blocks < 1 || n_reactions < 1 || n_total < 1)
+    return PYST_EINVAL;
+  return launch_score_combine(d_part, n_blocks, n_reactions, n_total, d_grad,
+                              (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -33,6 +33,7 @@ struct RunArgs {
   int64_t step_budget;
   int32_t ssa_fallback_steps;
   int32_t max_leap_retries;
+  int32_t stage_polls;  // bound of the model-staging wait (stage_blob)
 };
 
 // Output pointers of one trajectory (already offset to it).

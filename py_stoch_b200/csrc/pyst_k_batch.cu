@@ -133,9 +133,10 @@ __global__ void PYST_BATCH_BOUNDS
     const pyst_batch_item item = items[it];
     const uint32_t* blob = gblobs + item.blob_offset;
     const int words = (int)__ldg(blob + PYST_H_WORDS);
-    const bool ok = stage_blob(sblob, blob, words, bar, parity);
+    const bool ok = stage_blob(sblob, blob, words, bar, parity,
+                               ra.stage_polls);
     if (!ok) {
-      mbar_wait(bar, parity);
+      mbar_drain(bar, parity);
       for (int64_t u = threadIdx.x; u < item.n_traj; u += bs)
         mark_staging_failure(ob, item.traj_offset + u);
       break;
@@ -143,43 +144,61 @@ __global__ void PYST_BATCH_BOUNDS
     parity ^= 1u;
     ModelView m;
     m.load(sblob);
-    if (item.mapping == PYST_MAP_THREAD &&
-        packed_bytes(m.R) <= (size_t)pk_bytes) {
-      // (uniform over the block: every thread reads the same item)
-      m.pk = spk;
-      m.fast = __syncthreads_and(pack_reactions(m, spk)) != 0;
-    }
-    const bool tau = item.method == PYST_METHOD_TAU_LEAP;
-    if (item.mapping == PYST_MAP_THREAD) {
-      int32_t* xcol = (int32_t*)dyn + threadIdx.x;
-      int64_t* slot =
-          (int64_t*)((int32_t*)dyn + (size_t)m.S * bs) + threadIdx.x;
+    if (SCORE && ob.score && m.nlaw > 0) {
+      // (block-uniform) scores need a_j proportional to rate_j (mass
+      // action): the item is not simulated; its samples read -1 and its
+      // scores NaN
+      const int KF = m.kappa * m.ita;
+      const double nan = __longlong_as_double(0x7ff8000000000000ll);
       for (int64_t u = threadIdx.x; u < item.n_traj; u += bs) {
         const TrajOut o = ob.at(item.sample_offset, u, item.traj_offset,
                                 item.score_offset, item.n_traj, m.R);
-        const uint64_t id = (uint64_t)item.traj_id_base + (uint64_t)u;
-        if (m.R <= 8) {
-          if (tau) run_thread<8, true, SCORE>(m, xcol, slot, bs, ra, id, o);
-          else run_thread<8, false, SCORE>(m, xcol, slot, bs, ra, id, o);
-        } else if (SCORE || m.R <= PYST_THREAD_MAX_REACTIONS) {
-          // (the host maps scored items with more reactions to warps)
-          if (tau) run_thread<32, true, SCORE>(m, xcol, slot, bs, ra, id, o);
-          else run_thread<32, false, SCORE>(m, xcol, slot, bs, ra, id, o);
-        } else {
-          if (tau) run_thread_big<true>(m, xcol, slot, bs, ra, id, o);
-          else run_thread_big<false>(m, xcol, slot, bs, ra, id, o);
-        }
+        for (int kf = 0; kf < KF; ++kf) o.samples[(int64_t)kf * o.stride] = -1;
+        if (o.status) *o.status = (uint8_t)PYST_TRAJ_UNSUPPORTED;
+        if (o.events) *o.events = 0;
+        if (o.seqhash) *o.seqhash = 0;
+        if (o.t_final) *o.t_final = 0.0;
+        for (int j = 0; j < m.R; ++j) o.score[j] = nan;
       }
     } else {
-      unsigned char* mine = dyn + (size_t)wid * warp_bytes;
-      const WarpSmem ws = warp_smem(mine, m.S, m.R);
-      double* sacc = (double*)(mine + warp_smem_bytes(m.S, m.R));
-      for (int64_t u = wid; u < item.n_traj; u += nw) {
-        const TrajOut o = ob.at(item.sample_offset, u, item.traj_offset,
-                                item.score_offset, item.n_traj, m.R);
-        const uint64_t id = (uint64_t)item.traj_id_base + (uint64_t)u;
-        if (tau) run_warp<true, SCORE>(m, ws, ra, id, o, sacc);
-        else run_warp<false, SCORE>(m, ws, ra, id, o, sacc);
+      if (item.mapping == PYST_MAP_THREAD &&
+          packed_bytes(m.R) <= (size_t)pk_bytes) {
+        // (uniform over the block: every thread reads the same item)
+        m.pk = spk;
+        m.fast = __syncthreads_and(pack_reactions(m, spk)) != 0;
+      }
+      const bool tau = item.method == PYST_METHOD_TAU_LEAP;
+      if (item.mapping == PYST_MAP_THREAD) {
+        int32_t* xcol = (int32_t*)dyn + threadIdx.x;
+        int64_t* slot =
+            (int64_t*)((int32_t*)dyn + (size_t)m.S * bs) + threadIdx.x;
+        for (int64_t u = threadIdx.x; u < item.n_traj; u += bs) {
+          const TrajOut o = ob.at(item.sample_offset, u, item.traj_offset,
+                                  item.score_offset, item.n_traj, m.R);
+          const uint64_t id = (uint64_t)item.traj_id_base + (uint64_t)u;
+          if (m.R <= 8) {
+            if (tau) run_thread<8, true, SCORE>(m, xcol, slot, bs, ra, id, o);
+            else run_thread<8, false, SCORE>(m, xcol, slot, bs, ra, id, o);
+          } else if (SCORE || m.R <= PYST_THREAD_MAX_REACTIONS) {
+            // (the host maps scored items with more reactions to warps)
+            if (tau) run_thread<32, true, SCORE>(m, xcol, slot, bs, ra, id, o);
+            else run_thread<32, false, SCORE>(m, xcol, slot, bs, ra, id, o);
+          } else {
+            if (tau) run_thread_big<true>(m, xcol, slot, bs, ra, id, o);
+            else run_thread_big<false>(m, xcol, slot, bs, ra, id, o);
+          }
+        }
+      } else {
+        unsigned char* mine = dyn + (size_t)wid * warp_bytes;
+        const WarpSmem ws = warp_smem(mine, m.S, m.R);
+        double* sacc = (double*)(mine + warp_smem_bytes(m.S, m.R));
+        for (int64_t u = wid; u < item.n_traj; u += nw) {
+          const TrajOut o = ob.at(item.sample_offset, u, item.traj_offset,
+                                  item.score_offset, item.n_traj, m.R);
+          const uint64_t id = (uint64_t)item.traj_id_base + (uint64_t)u;
+          if (tau) run_warp<true, SCORE>(m, ws, ra, id, o, sacc);
+          else run_warp<false, SCORE>(m, ws, ra, id, o, sacc);
+        }
       }
     }
     if (ob.stats || ob.jac) {

@@ -47,15 +47,72 @@ __global__ void __launch_bounds__(PYST_BWD_CHUNK)
   }
 }
 
-__global__ void k_score_final(const double* __restrict__ part, int nblk, int R,
-                              int64_t U, double* grad) {
+__global__ void k_score_final(const double* __restrict__ part, int64_t nblk,
+                              int R, int64_t U, double* grad) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < R;
        j += gridDim.x * blockDim.x) {
     double acc = 0.0;
-    for (int b = 0; b < nblk; ++b)
-      acc = __dadd_rn(acc, part[(int64_t)b * R + j]);
+    for (int64_t b = 0; b < nblk; ++b)
+      acc = __dadd_rn(acc, part[b * R + j]);
     grad[j] = __ddiv_rn(acc, (double)U);
   }
+}
+
+// Exact integer sufficient statistics of sample rows: for row kf (of
+// kappa*ita) and the trajectories of this block's chunk, sum x, and x^2
+// split into its high and low 32-bit halves (x^2 < 2^62), all added with
+// 64-bit integer atomics into the zeroed sums[kf][3].  Integer sums are
+// exact, so the result does not depend on the order of the additions, on
+// the chunking or on how trajectories are split across GPUs.
+#define PYST_SUMS_CHUNK 4096
+__global__ void __launch_bounds__(256)
+    k_sample_sums(const int32_t* __restrict__ samples, int64_t U,
+                  int64_t stride, int rows, unsigned long long* sums) {
+  __shared__ unsigned long long red[3][256];
+  const int64_t u0 = (int64_t)blockIdx.x * PYST_SUMS_CHUNK;
+  const int64_t u1 = u0 + PYST_SUMS_CHUNK < U ? u0 + PYST_SUMS_CHUNK : U;
+  for (int kf = blockIdx.y; kf < rows; kf += gridDim.y) {
+    const int32_t* row = samples + (int64_t)kf * stride;
+    unsigned long long sx = 0, hi = 0, lo = 0;
+    for (int64_t u = u0 + threadIdx.x; u < u1; u += 256) {
+      const int64_t x = row[u];
+      const unsigned long long x2 = (unsigned long long)(x * x);
+      sx += (unsigned long long)x;  // two's complement: signed sum mod 2^64
+      hi += x2 >> 32;
+      lo += x2 & 0xFFFFFFFFull;
+    }
+    red[0][threadIdx.x] = sx;
+    red[1][threadIdx.x] = hi;
+    red[2][threadIdx.x] = lo;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+      if (threadIdx.x < w) {
+        red[0][threadIdx.x] += red[0][threadIdx.x + w];
+        red[1][threadIdx.x] += red[1][threadIdx.x + w];
+        red[2][threadIdx.x] += red[2][threadIdx.x + w];
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x < 3)
+      atomicAdd(sums + 3 * (int64_t)kf + threadIdx.x, red[threadIdx.x][0]);
+    __syncthreads();  // red is rewritten for the next row
+  }
+}
+
+// Population mean and variance of each row from its exact sums over n
+// trajectories: mean = sx / n, var = (hi 2^32 + lo) / n - mean^2.
+__global__ void k_moments_from_sums(const long long* __restrict__ sums,
+                                    int rows, int64_t n, double* mean,
+                                    double* var) {
+  const int kf = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kf >= rows) return;
+  const double dn = (double)n;
+  const double m = __ddiv_rn((double)sums[3 * kf], dn);
+  const double x2 = __dadd_rn(__dmul_rn((double)sums[3 * kf + 1],
+                                        4294967296.0),
+                              (double)sums[3 * kf + 2]);
+  mean[kf] = m;
+  var[kf] = __dsub_rn(__ddiv_rn(x2, dn), __dmul_rn(m, m));
 }
 
 __global__ void k_philox(uint64_t seed, uint64_t id, uint64_t n0,
@@ -122,7 +179,45 @@ int launch_score_backward(const int32_t* samples, const double* score,
   const int64_t nblk = score_backward_blocks(U);
   k_score_partial<<<(unsigned)nblk, PYST_BWD_CHUNK, 0, st>>>(
       samples, score, U, kappa, ita, R, mean, var, gmean, gvar, part);
-  k_score_final<<<(R + 127) / 128, 128, 0, st>>>(part, (int)nblk, R, U, grad);
+  k_score_final<<<(R + 127) / 128, 128, 0, st>>>(part, nblk, R, U, grad);
+  return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
+}
+
+int launch_score_partials(const int32_t* samples, const double* score,
+                          int64_t U, int kappa, int ita, int R,
+                          const double* mean, const double* var,
+                          const double* gmean, const double* gvar,
+                          double* part, cudaStream_t st) {
+  const int64_t nblk = score_backward_blocks(U);
+  k_score_partial<<<(unsigned)nblk, PYST_BWD_CHUNK, 0, st>>>(
+      samples, score, U, kappa, ita, R, mean, var, gmean, gvar, part);
+  return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
+}
+
+int launch_score_combine(const double* part, int64_t nblk, int R,
+                         int64_t n_total, double* grad, cudaStream_t st) {
+  k_score_final<<<(R + 127) / 128, 128, 0, st>>>(part, nblk, R, n_total,
+                                                 grad);
+  return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
+}
+
+int launch_sample_sums(const int32_t* samples, int64_t U, int64_t stride,
+                       int rows, int64_t* sums, cudaStream_t st) {
+  if (cudaMemsetAsync(sums, 0, (size_t)rows * 3 * sizeof(int64_t), st) !=
+      cudaSuccess)
+    return PYST_ECUDA;
+  if (U == 0) return PYST_OK;
+  const dim3 grid((unsigned)((U + PYST_SUMS_CHUNK - 1) / PYST_SUMS_CHUNK),
+                  (unsigned)(rows < 65535 ? rows : 65535));
+  k_sample_sums<<<grid, 256, 0, st>>>(samples, U, stride, rows,
+                                      (unsigned long long*)sums);
+  return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
+}
+
+int launch_moments_from_sums(const int64_t* sums, int rows, int64_t n,
+                             double* mean, double* var, cudaStream_t st) {
+  k_moments_from_sums<<<(rows + 127) / 128, 128, 0, st>>>(
+      (const long long*)sums, rows, n, mean, var);
   return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
 }
 

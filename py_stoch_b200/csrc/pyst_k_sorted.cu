@@ -200,7 +200,8 @@ __global__ void __launch_bounds__(kMaxBlock, kMinBlocks)
     fence_barrier_init();
   }
   __syncthreads();
-  const bool ok = stage_blob(sm.blob, gblob, blob_words, sm.bar, 0);
+  const bool ok = stage_blob(sm.blob, gblob, blob_words, sm.bar, 0,
+                             ra.stage_polls);
   // Initial fill: a balanced contiguous range per block when every
   // trajectory fits the pools, else full pools and the queue for the rest.
   const int64_t grid = gridDim.x;
@@ -211,7 +212,7 @@ __global__ void __launch_bounds__(kMaxBlock, kMinBlocks)
                           : ((int64_t)blockIdx.x + 1) * n_traj / grid;
   const int64_t qbase = full ? grid * slots : n_traj;
   if (!ok) {
-    mbar_wait(sm.bar, 0);
+    mbar_drain(sm.bar, 0);
     for (int k = 0; k < pool; ++k) {
       const int64_t u = lo + k * nb + tid;
       if (u < hi) mark_staging_failure(ob, u);

@@ -46,14 +46,15 @@ __global__ void __launch_bounds__(128, PYST_THREAD_MINB)
     fence_barrier_init();
   }
   __syncthreads();
-  const bool ok = stage_blob(sblob, gblob, blob_words, bar, 0);
+  const bool ok = stage_blob(sblob, gblob, blob_words, bar, 0,
+                             ra.stage_polls);
   const int bs = blockDim.x;
   const int64_t nthreads = (int64_t)gridDim.x * bs;
   // first trajectory by thread index, later ones from the shared queue, so
   // a thread whose trajectory ends early takes the next unstarted one
   int64_t u = blockIdx.x * (int64_t)bs + threadIdx.x;
   if (!ok) {
-    mbar_wait(bar, 0);  // let a late copy land before the block exits
+    mbar_drain(bar, 0);  // let a late copy land before the block exits
     while (u < n_traj) {
       mark_staging_failure(ob, u);
       u = nthreads + (int64_t)atomicAdd(queue, 1ull);
@@ -111,13 +112,14 @@ __global__ void __launch_bounds__(128)
     fence_barrier_init();
   }
   __syncthreads();
-  const bool ok = stage_blob(sblob, gblob, blob_words, bar, 0);
+  const bool ok = stage_blob(sblob, gblob, blob_words, bar, 0,
+                             ra.stage_polls);
   const int bs = blockDim.x;
   const int64_t ngroups = (int64_t)gridDim.x * bs / LG;
   const bool leader = (threadIdx.x & (LG - 1)) == 0;
   int64_t u = (blockIdx.x * (int64_t)bs + threadIdx.x) / LG;
   if (!ok) {
-    mbar_wait(bar, 0);  // let a late copy land before the block exits
+    mbar_drain(bar, 0);  // let a late copy land before the block exits
     for (; u < n_traj; u += ngroups)
       if (leader) mark_staging_failure(ob, u);
     return;

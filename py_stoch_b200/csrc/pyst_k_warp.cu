@@ -26,7 +26,8 @@ __global__ void __launch_bounds__(128)
   const int nw = blockDim.x >> 5, wid = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = (int64_t)gridDim.x * nw;
-  const bool ok = stage_blob(sblob, gblob, blob_words, bar, 0);
+  const bool ok = stage_blob(sblob, gblob, blob_words, bar, 0,
+                             ra.stage_polls);
   int64_t u = blockIdx.x * (int64_t)nw + wid;
   auto next = [&]() {
     long long v = 0;
@@ -34,7 +35,7 @@ __global__ void __launch_bounds__(128)
     return nwarps + (int64_t)__shfl_sync(0xffffffffu, v, 0);
   };
   if (!ok) {
-    mbar_wait(bar, 0);
+    mbar_drain(bar, 0);
     while (u < n_traj) {
       if (lane == 0) mark_staging_failure(ob, u);
       u = next();

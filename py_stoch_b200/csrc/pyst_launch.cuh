@@ -131,6 +131,17 @@ int launch_score_backward(const int32_t* samples, const double* score,
                           const double* gmean, const double* gvar,
                           double* part, double* grad, cudaStream_t st);
 int64_t score_backward_blocks(int64_t U);
+int launch_score_partials(const int32_t* samples, const double* score,
+                          int64_t U, int kappa, int ita, int R,
+                          const double* mean, const double* var,
+                          const double* gmean, const double* gvar,
+                          double* part, cudaStream_t st);
+int launch_score_combine(const double* part, int64_t nblk, int R,
+                         int64_t n_total, double* grad, cudaStream_t st);
+int launch_sample_sums(const int32_t* samples, int64_t U, int64_t stride,
+                       int rows, int64_t* sums, cudaStream_t st);
+int launch_moments_from_sums(const int64_t* sums, int rows, int64_t n,
+                             double* mean, double* var, cudaStream_t st);
 
 }  // namespace pyst
 

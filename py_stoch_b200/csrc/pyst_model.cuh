@@ -161,21 +161,31 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // Bounded wait: gives up after `limit` polls (each try_wait itself blocks
 // for a hardware-defined interval), so a lost completion cannot hang.
 #define PYST_MBAR_POLL_LIMIT (1 << 22)
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (int i = 0; i < PYST_MBAR_POLL_LIMIT; ++i)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          int limit) {
+  for (int i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
 
+// After a staging wait gave up: wait again, bounded, for the copy still in
+// flight, so it cannot land in shared memory that the block has moved on
+// from (or released by exiting).
+__device__ __forceinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {
+  return mbar_wait(bar, parity, PYST_MBAR_POLL_LIMIT);
+}
+
 // Stage `words` (multiple of 4) words of `src` into `dst` with one
 // bulk-async copy issued by thread 0; every thread of the block waits on
-// phase `parity` of `bar`.  Returns false on timeout, the same value in
-// every thread (a block-wide vote, so callers may branch on it around
-// barriers).  Must be called by all threads of the block.  `bar` must have
-// been initialised with count 1.
+// phase `parity` of `bar`, for at most `polls` polls (RunArgs.stage_polls).
+// Returns false on timeout, the same value in every thread (a block-wide
+// vote, so callers may branch on it around barriers); the caller then
+// drains the copy (mbar_drain) before reusing or releasing `dst`.  Must be
+// called by all threads of the block.  `bar` must have been initialised
+// with count 1.
 __device__ __forceinline__ bool stage_blob(uint32_t* dst, const uint32_t* src,
                                            int words, uint64_t* bar,
-                                           uint32_t parity) {
+                                           uint32_t parity, int polls) {
   if (threadIdx.x == 0) {
     // Order earlier generic-proxy reads of dst before the async write.
     fence_proxy_async();
@@ -183,7 +193,7 @@ __device__ __forceinline__ bool stage_blob(uint32_t* dst, const uint32_t* src,
     mbar_arrive_expect_tx(bar, bytes);
     bulk_g2s(dst, src, bytes, bar);
   }
-  return __syncthreads_and(mbar_wait(bar, parity)) != 0;
+  return __syncthreads_and(mbar_wait(bar, parity, polls)) != 0;
 }
 
 }  // namespace pyst

@@ -33,7 +33,7 @@ DEFAULT_STEP_BUDGET = 100_000_000
 
 ERROR_STATUSES = (_lib.TRAJ_STEP_BUDGET, _lib.TRAJ_OVERFLOW,
                   _lib.TRAJ_LEAP_RETRY, _lib.TRAJ_SAMPLER, _lib.TRAJ_STAGING,
-                  _lib.TRAJ_RATE)
+                  _lib.TRAJ_RATE, _lib.TRAJ_UNSUPPORTED)
 
 
 def _torch():

@@ -7,7 +7,7 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if REPO not in sys.path:
     sys.path.insert(0, REPO)
 
-from oracle.build_ref import DEFAULT_REF as REFERENCE  # noqa: E402
+from oracle.build_ref import reference_dir  # noqa: E402
 
 
 def pytest_configure(config):

@@ -37,9 +37,10 @@ def test_exports_every_declared_symbol(built_lib):
 def test_version_and_strings(built_lib):
     assert built_lib.pyst_abi_version() == 2
     for code in range(6):
-        assert built_lib.pyst_status_string(code)
-    for code in range(7):
-        assert built_lib.pyst_traj_status_string(code)
+        assert built_lib.pyst_status_string(code) != b'unknown status'
+    for code in range(9):
+        assert built_lib.pyst_traj_status_string(code) != (
+            b'unknown trajectory status')
 
 
 def _run_args():
@@ -99,6 +100,41 @@ def test_run_rejects_bad_arguments(built_lib):
     ws = C.c_size_t(0)
     assert L.pyst_run_workspace_size(C.byref(r), C.byref(ws)) == 0
     assert ws.value == _lib.RUN_WORKSPACE_BYTES
+
+
+def _law_model():
+    """Birth-death whose death hazard is the general law k1 * |x|."""
+    from py_stoch_b200 import kinetic
+    from py_stoch_b200.model import Model
+    code, consts, _ = kinetic.compile_law('parameter_1 * abs(species_0)', 1,
+                                          [2000.0, 0.5])
+    return Model([[0, 0]], [[0, 1]], [[1, -1]], [2000.0, 0.0], [0],
+                 np.linspace(0, 1, 5).astype(np.float32), [0],
+                 laws=[None, (code, consts)])
+
+
+def test_scores_refused_for_general_laws(built_lib):
+    """N_j - int a_j dt is d log p / d log rate_j only for mass action: the
+    run calls refuse scores for a model with a general kinetic law (before
+    any CUDA call), and accept the same call without scores."""
+    L = built_lib
+    m = _law_model()
+    assert m.has_laws
+    blob = m.blob()
+    r, o = _run_args()
+    o.samples = 4096
+    o.score = 4096
+    for fn, meth in ((L.pyst_ssa_direct_run, 0), (L.pyst_tau_leap_run, 1)):
+        r.method = meth
+        assert fn(blob.ctypes.data, 16, C.byref(r), C.byref(o), 8, 256,
+                  None) == _lib.PYST_EUNSUPPORTED
+    # n_traj 0 with scores is refused too; without scores it is a no-op
+    r.n_traj = 0
+    assert L.pyst_tau_leap_run(blob.ctypes.data, 16, C.byref(r), C.byref(o),
+                               8, 256, None) == _lib.PYST_EUNSUPPORTED
+    o.score = 0
+    assert L.pyst_tau_leap_run(blob.ctypes.data, 16, C.byref(r), C.byref(o),
+                               8, 256, None) == _lib.PYST_OK
 
 
 def test_batch_and_backward_reject(built_lib):

@@ -7,7 +7,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import REFERENCE, reference_available
+from conftest import reference_available, reference_dir
 from py_stoch_b200 import parser, petri_net, sbml, sim_maker, simulator
 
 GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), 'golden',
@@ -25,7 +25,7 @@ def _fixture_model(fx):
         return sbml.read_sbml_string(sbml.schlogl_sbml())
     if not reference_available():
         pytest.skip('fixture XML only in the reference checkout')
-    return sbml.read_sbml(os.path.join(REFERENCE, 'examples', fx))
+    return sbml.read_sbml(os.path.join(reference_dir(), 'examples', fx))
 
 
 @pytest.mark.parametrize('fx', sorted(GOLDEN['fixtures']))

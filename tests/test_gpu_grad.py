@@ -19,7 +19,7 @@ from py_stoch_b200 import networks
 
 pytestmark = pytest.mark.gpu
 
-U = 262144
+U = 1048576  # the benchmarked gradient configuration
 
 
 @pytest.fixture(scope='module')

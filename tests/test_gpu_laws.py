@@ -116,3 +116,40 @@ def test_scores_refused_for_laws(torch_cuda, built_lib):
     from py_stoch_b200.simulator import simulate
     with pytest.raises(ValueError):
         simulate(_models()['saturating'], 32, score=True)
+
+
+def test_batched_scores_refused_for_laws(torch_cuda, built_lib):
+    """A scored batched launch (the C ABI, bypassing the Python guard) does
+    not simulate an item whose model has general kinetic laws: its
+    trajectories read PYST_TRAJ_UNSUPPORTED with samples -1 and NaN scores,
+    while the mass-action item of the same launch runs normally."""
+    import ctypes as C
+
+    from py_stoch_b200 import _lib, networks
+    from py_stoch_b200.batch import Batch
+    torch = torch_cuda
+    law = _models()['saturating']
+    ma = networks.telegraph(t_end=2.0, n_samples=5)
+    b = Batch([ma, law], 64, method='direct', order='given')
+    R = max(ma.n_reactions, law.n_reactions)
+    score = torch.full((2 * 64 * R,), 7.0, dtype=torch.float64,
+                       device='cuda')
+    o = b.out
+    outs = _lib.Outputs(o['samples'].data_ptr(), 0, o['status'].data_ptr(),
+                        o['events'].data_ptr(), 0, 0, score.data_ptr(), 0, 0)
+    r = _lib.RunDesc(0, 0, 5, 0, 0, 100, 63, 0, 0, 0)
+    L = built_lib
+    s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.pyst_batch_run(b.d_blobs.data_ptr(), b.d_items.data_ptr(), 2,
+                            C.byref(b.limits), C.byref(r), C.byref(outs),
+                            b.workspace.data_ptr(), b.workspace.numel(),
+                            s) == 0
+    torch.cuda.synchronize()
+    st = b.per_traj('status', 1).cpu().numpy()
+    assert (st == _lib.TRAJ_UNSUPPORTED).all()
+    assert (b.samples(1).cpu().numpy() == -1).all()
+    sc = score.cpu().numpy()
+    a = int(b.score_offset[1])
+    assert np.isnan(sc[a:a + 64 * law.n_reactions]).all()
+    assert (b.per_traj('status', 0).cpu().numpy() == 0).all()
+    assert np.isfinite(sc[:64 * ma.n_reactions]).all()
