@@ -223,6 +223,55 @@ class Batch(object):
         torch.cuda.current_stream(self.device).wait_stream(s)
         return g
 
+    @classmethod
+    def from_tl_args_list(cls, tl_args_list, simulator='tau', **kw):
+        """One batch for a whole sweep built by
+        :meth:`py_stoch_b200.sim_maker.TLArgsList.make_list`.
+
+        The reference runs such a list one point at a time, one
+        ``CuTauLeaping().run(args)`` (or ``CuGillespie().run(args)``) each
+        (``examples/schlogl_sim.py:66-80``).  Item i here is point i: its
+        ``args.U`` is rounded up by the same ``calculate_sizes`` rule (the
+        side effect the drop-in classes keep), it takes the direct method
+        when ``args.gillespie`` is set (or ``simulator='gillespie'``) and
+        tau-leaping otherwise, and -- like every point of the per-point loop
+        -- its trajectories have Philox ids 0..U-1.  With the same seed each
+        item's samples equal that point's ``run(args)`` result bit for bit
+        (:meth:`results` returns them as NumPy arrays).  Keyword arguments
+        go to :class:`Batch`."""
+        from .model import Model
+        from .simulator import CuGillespie, CuTauLeaping
+        sim = CuGillespie() if simulator == 'gillespie' else CuTauLeaping()
+        models, n_traj, methods = [], [], []
+        for args in tl_args_list:
+            sim.calculate_sizes(args)
+            models.append(Model.from_tl_args(args))
+            n_traj.append(int(args.U))
+            direct = simulator == 'gillespie' or getattr(args, 'gillespie',
+                                                         0)
+            methods.append('direct' if direct else 'tau')
+        kw.setdefault('traj_id_base', np.zeros(len(models), np.int64))
+        return cls(models, n_traj, method=methods, **kw)
+
+    def results(self):
+        """Per item, its samples ``[kappa, ita, n_traj]`` as int32 NumPy
+        arrays (the drop-in ``run(args)`` layout); raises if any trajectory
+        ended with an error status, as the drop-in classes do."""
+        torch = _torch()
+        torch.cuda.synchronize(self.device)
+        if 'status' in self.out:
+            from .simulator import ERROR_STATUSES
+            st = self.out['status'].cpu().numpy()
+            bad = np.isin(st, ERROR_STATUSES)
+            if bad.any():
+                L = _lib.lib()
+                codes = sorted(set(int(c) for c in st[bad]))
+                raise RuntimeError('%d of %d trajectories failed (%s)' % (
+                    int(bad.sum()), st.size, ', '.join(
+                        L.pyst_traj_status_string(c).decode()
+                        for c in codes)))
+        return [self.samples(i).cpu().numpy() for i in range(len(self.models))]
+
     # ---- per-item views -------------------------------------------------
     def samples(self, i):
         a = int(self.sample_offset[i])

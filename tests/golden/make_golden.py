@@ -44,6 +44,7 @@ FIXTURES = ['lotkaVoltera_sbml.xml', 'schlogl_sbmlv2.xml', 'schlogl_sbml.xml',
 
 def _py3(src):
     src = src.replace('.iteritems()', '.items()')
+    src = re.sub(r'except (\w+), (\w+):', r'except \1 as \2:', src)
     src = re.sub(r'string\.replace\(', '_py2_replace(', src)
     src = re.sub(r'^(\s*)print (?!\()(.*)$', r'\1print(\2)', src,
                  flags=re.M)
@@ -166,6 +167,46 @@ def _j(v):
     return v
 
 
+class _FixedNow(object):
+    """Stands in for datetime in the reference's saver: a fixed stamp."""
+    @staticmethod
+    def now():
+        import datetime
+        return datetime.datetime(2024, 5, 6, 7, 8)
+
+
+def saver_golden(ref, R):
+    """Run the reference's save_results (mod/utils/saver.py) on one sweep
+    point and a small deterministic result; record every file it writes
+    (path under the working directory, text content)."""
+    import tempfile
+    saver = _load(os.path.join(ref, 'mod/utils/saver.py'), 'ref_saver')
+    saver.datetime = _FixedNow
+    model = fake_libsbml.read_sbml(os.path.join(ref, 'examples',
+                                                'lotkaVoltera_sbml.xml'))
+    args = R['sim_maker'].TLArgsList.make_list(
+        model, [[1000], [900], [1]], [[10], [0.01], [10]], [0, 1], 10, 4,
+        3)[0]
+    result = (numpy.arange(2 * 4 * 3, dtype=numpy.int32).reshape(2, 4, 3)
+              * 37 % 1001)
+    cwd = os.getcwd()
+    files = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        os.chdir(tmp)
+        try:
+            saver.save_results(result, args, 'lv_run')
+        finally:
+            os.chdir(cwd)
+        for root, _, names in os.walk(tmp):
+            for n in names:
+                p = os.path.join(root, n)
+                with open(p) as f:
+                    files[os.path.relpath(p, tmp)] = f.read()
+    return {'result': _j(result), 'x_0': _j(args.x_0), 'c': _j(args.c),
+            'E': _j(args.E), 't_max': _j(args.t_max), 'ita': _j(args.ita),
+            'U': _j(args.U), 'files': files}
+
+
 def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
     R = load_reference(ref)
@@ -237,6 +278,8 @@ def main():
                 except ZeroDivisionError:
                     rec['error'] = 'ZeroDivisionError'
                 out['calculate_sizes'].append(rec)
+
+    out['saver'] = saver_golden(ref, R)
 
     path = os.path.join(HERE, 'frontend_golden.json')
     with open(path, 'w') as f:
