@@ -137,28 +137,6 @@ class ClockSampler(object):
                 'reasons': sorted(reasons), 'samples': len(sm)}
 
 
-def cpu_baseline(wl, target_s=12.0, threads=0):
-    """Oracle port on host cores over a bounded sample of the workload."""
-    from oracle import oracle
-    m, meth = wl['model'], 0 if wl['method'] == 'direct' else 1
-    n = wl['cpu_pilot']
-    t0 = time.perf_counter()
-    r = oracle.simulate(m, n, meth, seed=0, threads=threads)
-    dt = time.perf_counter() - t0
-    if dt < target_s / 4:
-        n2 = int(min(wl['n'], max(n, n * target_s / max(dt, 1e-3))))
-        t0 = time.perf_counter()
-        r = oracle.simulate(m, n2, meth, seed=1, threads=threads)
-        dt = time.perf_counter() - t0
-        n = n2
-    ev = float(r['events'].sum())
-    cores = threads if threads > 0 else oracle.max_threads()
-    return {'value': ev / dt, 'unit': UNIT, 'cores': cores, 'kind': 'port',
-            'sample': '%d of %d trajectories of the same workload, %.1f s'
-                      % (n, wl['n'], dt),
-            'trajectories_per_s': n / dt}
-
-
 def expected_events(wl, n=2048):
     """Mean reaction firings per trajectory of the workload, from the CPU
     oracle (same law as the reference; the reference kernels do not count
@@ -289,6 +267,19 @@ def completed_events(events, status):
     return float(events[status <= 1].sum().item())
 
 
+def _form_record(ms, events, ok_events, status_counts, n_models, n_traj,
+                 launches):
+    st = [int(c) for c in status_counts]
+    tot = float(sum(st))
+    return {'ms': ms, 'models': n_models, 'launches': launches,
+            'events': events, 'events_per_s': events / ms * 1e3,
+            'completed_events_per_s': ok_events / ms * 1e3,
+            'trajectories_per_s': n_models * n_traj / ms * 1e3,
+            'status_counts': st,
+            'unfinished_fraction': st[2] / tot if tot else 0.0,
+            'error_fraction': sum(st[2:]) / tot if tot else 0.0}
+
+
 def batch_vs_plain(kind, dev, subset=256, steps=1, full=True, budget=20000):
     """Events/s of the batched form (one persistent launch, CUDA graph) and
     of the plain form (one launch per model) on the same models.
@@ -299,7 +290,11 @@ def batch_vs_plain(kind, dev, subset=256, steps=1, full=True, budget=20000):
     (batched+grad).  kind 'synthetic': 4096 uneven synthetic networks, 64
     trajectories each, tau-leaping.  Both forms run the same trajectories
     with the same step budget and produce identical per-trajectory results;
-    only the scheduling differs."""
+    only the scheduling differs.  `completed_events_per_s` counts the
+    firings of trajectories that reached t_end or absorption; trajectories
+    stopped by the step budget are reported as `unfinished_fraction`, and
+    int32 overflows (Lotka-Volterra sets whose prey grows without bound)
+    in `status_counts`."""
     import torch
     from py_stoch_b200 import networks
     from py_stoch_b200.autotune import Autotuner
@@ -331,19 +326,19 @@ def batch_vs_plain(kind, dev, subset=256, steps=1, full=True, budget=20000):
                   device=dev, score=grad, stats=grad, jacobian=grad,
                   traj_id_base=ids)
         g = b.graph(seed=11, step_budget=budget)
-        g.replay()
         tot_ms, ev, ev_ok = 0.0, 0.0, 0.0
         for _ in range(steps):
             ms_, _ = _events_timed(g.replay, stream)
             tot_ms += ms_
             ev += float(b.out['events'].sum().item())
             ev_ok += completed_events(b.out['events'], b.out['status'])
-        st = torch.bincount(b.out['status'].long(), minlength=7).tolist()
+        st = torch.bincount(b.out['status'].long(), minlength=9).tolist()
         del g
-        return tot_ms / steps, ev / steps, st, b, ev_ok / steps
+        return _form_record(tot_ms / steps, ev / steps, ev_ok / steps, st,
+                            len(ms), n_traj, 1)
 
     ids = [i * n_traj for i in pick]
-    ms_b, ev_b, st_b, _, ok_b = batched(sub, ids)
+    res['batched_same_models'] = batched(sub, ids)
     # plain form: one simulate() launch per model, same ids and budget
     outs = [{'samples': torch.empty((m.kappa, m.ita, n_traj),
                                     dtype=torch.int32, device=dev),
@@ -359,78 +354,177 @@ def batch_vs_plain(kind, dev, subset=256, steps=1, full=True, budget=20000):
                      step_budget=budget,
                      mapping=('thread' if tuner.mapping(m, 'tau') == 1
                               else 'warp'))
-    plain()
     ms_p, _ = _events_timed(plain, stream)
     ev_p = float(sum(int(o['events'].sum().item()) for o in outs))
     ok_p = sum(completed_events(o['events'], o['status']) for o in outs)
-    res['plain'] = {'ms': ms_p, 'events': ev_p, 'events_per_s':
-                    ev_p / ms_p * 1e3, 'completed_events_per_s':
-                    ok_p / ms_p * 1e3, 'launches': len(sub)}
-    res['batched_same_models'] = {'ms': ms_b, 'events': ev_b,
-                                  'events_per_s': ev_b / ms_b * 1e3,
-                                  'completed_events_per_s':
-                                      ok_b / ms_b * 1e3,
-                                  'launches': 1, 'status_counts': st_b}
-    res['batched_over_plain'] = (ev_b / ms_b) / (ev_p / ms_p)
+    st_p = np.sum([torch.bincount(o['status'].long(), minlength=9).tolist()
+                   for o in outs], axis=0)
+    res['plain'] = _form_record(ms_p, ev_p, ok_p, st_p, len(sub), n_traj,
+                                len(sub))
+    bs = res['batched_same_models']
+    res['batched_over_plain'] = bs['events_per_s'] / res['plain'][
+        'events_per_s']
+    res['batched_over_plain_completed'] = (
+        bs['completed_events_per_s'] /
+        max(res['plain']['completed_events_per_s'], 1e-30))
+    res['same_results'] = bool(bs['events'] == ev_p and bs[
+        'status_counts'] == res['plain']['status_counts'])
     if full:
-        ms_f, ev_f, st_f, b, ok_f = batched(models)
-        res['batched_full'] = {'models': len(models), 'ms': ms_f,
-                               'events': ev_f,
-                               'events_per_s': ev_f / ms_f * 1e3,
-                               'completed_events_per_s': ok_f / ms_f * 1e3,
-                               'trajectories_per_s':
-                                   len(models) * n_traj / ms_f * 1e3,
-                               'status_counts': st_f}
-        del b
+        res['batched_full'] = batched(models)
     res['autotune'] = {k: v['mapping'] for k, v in tuner.table.items()
                        if 'mapping' in v}
     torch.cuda.empty_cache()
     return res
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=5)
-    ap.add_argument('--warmup', type=int, default=3)
-    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--workload', default='schlogl_tau')
-    ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--n-traj', type=int, default=0,
-                    help='override trajectories per GPU (profiling runs)')
-    ap.add_argument('--no-forms', action='store_true',
-                    help='skip the batched-vs-plain comparison')
-    args = ap.parse_args()
-    if args.workload in ('sweep', 'synthetic'):
-        return forms_main(args)
-    wl = workloads()[args.workload]
-    if args.n_traj:
-        wl['n'] = args.n_traj
-    if args.impl == 'reference':
-        return run_reference(args, wl)
+# ---------------------------------------------------------------------------
+# instruction roofline: measured pipe peaks and algorithmic operations
+# ---------------------------------------------------------------------------
+PIPES = ('int32', 'fp32', 'fp64')
 
+
+def measure_pipe_peaks(dev, reps=3):
+    """Issue rates of the arithmetic pipes on this GPU, measured now with
+    the library's probe kernel (pyst_test_pipe: 8 independent chains per
+    thread, 8 blocks of 256 threads per SM), CUDA events on the launching
+    stream, best of `reps`.  Operations per second: an FMA counts one."""
+    import ctypes as C
+
+    import torch
+
+    from py_stoch_b200 import _lib
+    L = _lib.lib()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    blocks, iters = sms * 8, 2048
+    sink = torch.empty(blocks * 256, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = C.c_void_p(stream.cuda_stream)
+    rates = {}
+    for which, name, per in ((0, 'fp32_fma', 1), (1, 'int32_mad', 1),
+                             (2, 'fp64_fma', 1), (3, 'int32_alu', 2)):
+        best = 0.0
+        for r in range(reps + 1):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            _lib.check(L.pyst_test_pipe(which, iters, blocks,
+                                        sink.data_ptr(), sp),
+                       'pyst_test_pipe')
+            b.record(stream)
+            b.synchronize()
+            if r:  # the first launch is a warm-up
+                ops = 8.0 * per * iters * 256 * blocks
+                best = max(best, ops / (a.elapsed_time(b) * 1e-3))
+        rates[name] = best
+    # Philox's multiplies run on the multiply-add pipe, its xors and key
+    # additions on the ALU pipe; the larger of the two rates is the INT32
+    # denominator (the less flattering choice if both pipes issue at once)
+    return {'int32': max(rates['int32_mad'], rates['int32_alu']),
+            'fp32': rates['fp32_fma'], 'fp64': rates['fp64_fma'],
+            'probes': rates}
+
+
+# Operation counts of this engine's building blocks (pyst_math.cuh,
+# pyst_engine.cuh), counted from their arithmetic: an FMA, add, multiply,
+# divide, compare or conversion is one operation.
+PHILOX_INT = 98      # 10 rounds x (2 mul.lo + 2 mul.hi + 4 xor) + 9 x 2 key adds
+U53_INT = 2          # 53-bit uniform: shift, or
+LOG64 = 22           # pyst_log: split, (f-1)/(f+1), 11-term series, scaling
+EXP64 = 20           # pyst_exp: reduction, 15-term series, scaling
+
+
+def ops_per_trajectory(model, mix, tau, grad=False, fallback=100):
+    """Algorithmic operations per trajectory, by pipe, of this engine's
+    method on `model`, given the measured per-trajectory step mix (means of
+    the oracle's counters: SSA steps, leaps, inversion Poisson draws and
+    their search iterations, PTRS draws and their iterations).
+
+    SSA step: one Philox block and two 53-bit uniforms, the FP32
+    propensities (one multiply per reactant factor), the FP64 total and
+    cumulative selection (2M), tau = e/a0, r = u a0 and the clock add, one
+    log; the fired reaction's net changes.  A DECIDE (before every leap and
+    every SSA fallback round): propensities, the critical-reaction test,
+    the leap mean/variance sums (4 FP32 per net-change entry) and the tau
+    candidate of each reactant species (8 FP32).  A leap: its Poisson
+    draws (inversion: one Philox block, an exp, 3 FP64 per search step;
+    PTRS: 12 FP32 set-up, half a Philox block and 11 FP32 per iteration),
+    the state update and the critical-reaction clock.  Scores add, per SSA
+    step, an FP64 multiply-add per reaction and an integer count."""
+    M, S = model.n_reactions, model.n_species
+    order = np.asarray(model.order).sum(axis=0).astype(float)
+    nnz = (np.asarray(model.net) != 0).sum(axis=0).astype(float)
+    nneg = float((np.asarray(model.net) < 0).sum())
+    react = float((np.asarray(model.hor) > 0).sum())
+    prop32 = float(order.sum())
+    ssa, leaps = mix['ssa'], mix['leaps']
+    ops = {p: 0.0 for p in PIPES}
+
+    def add(n, i=0.0, f32=0.0, f64=0.0):
+        ops['int32'] += n * i
+        ops['fp32'] += n * f32
+        ops['fp64'] += n * f64
+
+    add(ssa, i=PHILOX_INT + 2 * U53_INT + nnz.mean(), f32=prop32,
+        f64=2 * M + 3 + 2 + LOG64)
+    if grad:
+        add(ssa, i=1, f64=2 * M)
+    if tau:
+        n_decide = leaps + ssa / float(fallback)
+        add(n_decide, i=2 * nneg, f32=prop32 + 4 * nnz.sum() + 8 * react,
+            f64=M + 1)
+        add(leaps, i=2 * nnz.sum() + S, f64=M + 3)
+        add(mix['inv_draws'], i=PHILOX_INT + 1, f64=EXP64 + 2)
+        add(mix['inv_iters'], f64=3)
+        add(mix['ptrs_draws'], f32=12)
+        add(mix['ptrs_iters'], i=PHILOX_INT / 2.0, f32=11)
+    return ops
+
+
+def step_mix(oracle_result):
+    """Per-trajectory means of the oracle's step counters and firings."""
+    st = oracle_result['steps'].astype(np.float64)
+    names = ('ssa', 'leaps', 'inv_draws', 'inv_iters', 'ptrs_draws',
+             'ptrs_iters')
+    mix = {k: float(st[:, q].mean()) for q, k in enumerate(names)}
+    mix['events'] = float(oracle_result['events'].astype(np.float64).mean())
+    return mix
+
+
+def ops_roofline(events_per_s, model, mix, peaks, tau, grad=False):
+    """The instruction roofline of a simulation: algorithmic operations per
+    event on each pipe x events/s against the measured pipe peak; the bound
+    is the pipe with the largest fraction."""
+    per_traj = ops_per_trajectory(model, mix, tau, grad)
+    per_event = {p: per_traj[p] / mix['events'] for p in PIPES}
+    pipes = {}
+    for p in PIPES:
+        a = events_per_s * per_event[p]
+        pipes[p] = {'achieved_gops': a / 1e9, 'peak_gops': peaks[p] / 1e9,
+                    'frac': a / peaks[p]}
+    bound = max(PIPES, key=lambda p: pipes[p]['frac'])
+    return {'bound': 'issue', 'pipe': bound,
+            'achieved': pipes[bound]['achieved_gops'],
+            'peak': pipes[bound]['peak_gops'], 'unit': 'Gop/s',
+            'frac': pipes[bound]['frac'], 'peak_source': 'measured now '
+            '(pyst_test_pipe probe on this GPU)',
+            'algorithmic_ops_per_event': per_event,
+            'step_mix_per_trajectory': mix, 'pipes': pipes}
+
+
+# ---------------------------------------------------------------------------
+# plain single-model workloads
+# ---------------------------------------------------------------------------
+def run_plain(wl, steps, warmup, dev, world=1, rank=0, e2e=True):
+    """Time `steps` simulations of workload `wl` (one kernel launch each,
+    plus the score reduction for gradient workloads) after `warmup`
+    untimed ones; L2 flushed before every step; device time by CUDA events
+    on the launching stream, max over ranks.  With `e2e`, the same again
+    through the public API with the model blob copied in from pinned host
+    memory and the outputs copied back inside the timed region."""
     import torch
     import torch.distributed as dist
 
-    from py_stoch_b200 import build as _build
     from py_stoch_b200.simulator import simulate
-
-    world = int(os.environ.get('WORLD_SIZE', '1'))
-    rank = int(os.environ.get('RANK', '0'))
-    local = int(os.environ.get('LOCAL_RANK', '0'))
-    if world > 1:
-        import datetime
-        torch.cuda.set_device(local)
-        dist.init_process_group('nccl',
-                                timeout=datetime.timedelta(seconds=120))
-    dev = torch.device('cuda', local)
-    torch.cuda.set_device(dev)
-    # one rank (re)builds the library if its sources changed; the others
-    # wait, so no two processes compile into the same build directory
-    if rank == 0:
-        _build.build()
-    if world > 1:
-        dist.barrier()
     m, n, meth = wl['model'], wl['n'], wl['method']
     base = rank * n
     stream = torch.cuda.current_stream(dev)
@@ -457,17 +551,17 @@ def main():
                                          var, ones, ones, stream=stream)
         return res
 
-    for w in range(args.warmup):
+    for w in range(warmup):
         step(10_000 + w)
     torch.cuda.synchronize(dev)
-    clk = ClockSampler(local)
+    clk = ClockSampler(dev.index or 0)
     clk.start()
-    total_ms, events = 0.0, 0
-    errs = 0
+    total_ms, events, errs = 0.0, 0, 0
+    status_counts = np.zeros(9, np.int64)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
-    for s in range(args.steps):
+    for s in range(steps):
         flush.fill_(s & 0xFF)
         st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(
             enable_timing=True)
@@ -477,24 +571,33 @@ def main():
         en.synchronize()
         total_ms += st.elapsed_time(en)
         events += int(res['events'].sum().item())
-        errs += int((res['status'] >= 2).sum().item())
+        status_counts += np.bincount(res['status'].cpu().numpy(),
+                                     minlength=9)[:9]
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
     clocks = clk.stop()
-    t = torch.tensor([total_ms, float(events), float(errs)], dtype=torch.float64,
-                     device=dev)
+    errs = int(status_counts[2:].sum())
+    t = torch.tensor([total_ms, float(events), float(errs)],
+                     dtype=torch.float64, device=dev)
     if world > 1:
         tm = t[:1].clone()
         dist.all_reduce(tm, op=dist.ReduceOp.MAX)
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         t[0] = tm[0]
     total_ms, events, errs = float(t[0]), float(t[1]), float(t[2])
-    sec = total_ms / 1e3
-    value = events / sec
-
+    r = {'ms_per_step': total_ms / steps, 'events_per_step': events / steps,
+         'value': events / (total_ms / 1e3),
+         'trajectories_per_s': n * world * steps / (total_ms / 1e3),
+         'error_trajectories': int(errs), 'clocks': clocks,
+         'status_counts': status_counts.tolist(),
+         'gpu_launches': steps * (5 if grad else 1),
+         'out_bytes': sum(v.numel() * v.element_size()
+                          for v in out.values())}
+    if not e2e:
+        return r
     # end to end through the public API: pinned host model blob in, samples
-    # and per-trajectory status/events out, every step
+    # and per-trajectory status/events (and the gradient) out, every step
     blob = torch.from_numpy(m.blob().view(np.int32)).pin_memory()
     d_blob = torch.empty_like(blob, device=dev)
     h_out = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
@@ -502,13 +605,15 @@ def main():
     h_grad = torch.empty(m.n_reactions, dtype=torch.float64,
                          pin_memory=True)
     e2e_ms, e2e_ev = 0.0, 0
-    for s in range(args.steps):
+    seed = None
+    for s in range(steps):
         flush.fill_(s & 0xFF)
         st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(
             enable_timing=True)
+        seed = 100 + s
         st.record(stream)
         d_blob.copy_(blob, non_blocking=True)
-        res = step(100 + s, d_blob=d_blob)
+        res = step(seed, d_blob=d_blob)
         for k in h_out:
             h_out[k].copy_(out[k], non_blocking=True)
         if grad:
@@ -517,74 +622,212 @@ def main():
         en.synchronize()
         e2e_ms += st.elapsed_time(en)
         e2e_ev += int(h_out['events'].sum())
-    e2 = torch.tensor([e2e_ms, float(e2e_ev)], dtype=torch.float64, device=dev)
+    e2 = torch.tensor([e2e_ms, float(e2e_ev)], dtype=torch.float64,
+                      device=dev)
     if world > 1:
         tm = e2[:1].clone()
         dist.all_reduce(tm, op=dist.ReduceOp.MAX)
         dist.all_reduce(e2, op=dist.ReduceOp.SUM)
         e2[0] = tm[0]
-    e2e_value = float(e2[1]) / (float(e2[0]) / 1e3)
-    h2d = blob.numel() * 4
     d2h = sum(v.numel() * v.element_size() for v in h_out.values())
-    if grad:
-        d2h += h_grad.numel() * 8
+    r['e2e'] = {'value': float(e2[1]) / (float(e2[0]) / 1e3), 'unit': UNIT,
+                'h2d_bytes_per_step': blob.numel() * 4,
+                'd2h_bytes_per_step': d2h + (h_grad.numel() * 8 if grad
+                                             else 0)}
+    # the last end-to-end step's host outputs, for the CPU check
+    r['_last'] = {'seed': seed, 'base': base, 'samples':
+                  h_out['samples'].numpy(), 'events':
+                  h_out['events'].numpy()}
+    return r
 
+
+def cpu_baseline(wl, check=None, target_s=12.0, threads=0):
+    """The oracle port on host cores over a bounded sample of the workload
+    (all of it when that fits ~`target_s`), which also gives the step mix
+    of the instruction roofline.  With `check` (the last end-to-end step's
+    seed, id base and host samples) the sample reruns exactly those
+    trajectories, so the bench's own GPU output is compared with the oracle
+    bit for bit."""
+    from oracle import oracle
+    m, meth = wl['model'], 0 if wl['method'] == 'direct' else 1
+    seed = check['seed'] if check else 1
+    base = check['base'] if check else 0
+    n = wl['cpu_pilot']
+    t0 = time.perf_counter()
+    r = oracle.simulate(m, wl['n'], meth, seed=seed, traj_id_base=base,
+                        threads=threads, u1=n)
+    dt = time.perf_counter() - t0
+    if dt < target_s / 4:
+        n = int(min(wl['n'], max(n, n * target_s / max(dt, 1e-3))))
+        t0 = time.perf_counter()
+        r = oracle.simulate(m, wl['n'], meth, seed=seed, traj_id_base=base,
+                            threads=threads, u1=n)
+        dt = time.perf_counter() - t0
+    part = {'samples': r['samples'][:, :, :n], 'events': r['events'][:n],
+            'steps': r['steps'][:n]}
+    ev = float(part['events'].sum())
+    cores = threads if threads > 0 else oracle.max_threads()
+    res = {'value': ev / dt, 'unit': UNIT, 'cores': cores, 'kind': 'port',
+           'sample': '%d of %d trajectories of the same workload, %.1f s'
+                     % (n, wl['n'], dt),
+           'trajectories_per_s': n / dt}
+    if check:
+        res['bench_output_checked'] = {
+            'trajectories': n,
+            'bit_exact': bool(np.array_equal(
+                part['samples'], check['samples'][:, :, :n]) and
+                np.array_equal(part['events'], check['events'][:n]))}
+    return res, step_mix(part)
+
+
+def plain_record(name, wl, args, dev, peaks, steps, warmup, world=1,
+                 rank=0):
+    """One workload's numbers: device-timed value, e2e, the instruction
+    roofline and, on one GPU, the CPU baseline with the output check."""
+    r = run_plain(wl, steps, warmup, dev, world, rank)
+    last = r.pop('_last', None)
+    rec = {'workload': wl['desc'], 'trajectories_per_gpu': wl['n']}
+    rec.update(r)
+    if world == 1 and not args.no_cpu_baseline:
+        cb, mix = cpu_baseline(wl, check=last)
+        rec['cpu_baseline'] = cb
+        rec['roofline'] = ops_roofline(r['value'] / world, wl['model'], mix,
+                                       peaks, wl['method'] == 'tau',
+                                       bool(wl.get('grad')))
+    return rec
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--workload', default='schlogl_tau')
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--n-traj', type=int, default=0,
+                    help='override trajectories per GPU (profiling runs)')
+    ap.add_argument('--no-configs', action='store_true',
+                    help='headline only: skip the other configurations')
+    args = ap.parse_args()
+    if args.workload in ('sweep', 'synthetic'):
+        return forms_main(args)
+    wl = workloads()[args.workload]
+    if args.n_traj:
+        wl['n'] = args.n_traj
+    if args.impl == 'reference':
+        return run_reference(args, wl)
+
+    import torch
+    import torch.distributed as dist
+
+    from py_stoch_b200 import build as _build
+
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl',
+                                timeout=datetime.timedelta(seconds=120))
+    dev = torch.device('cuda', local)
+    torch.cuda.set_device(dev)
+    # one rank (re)builds the library if its sources changed; the others
+    # wait, so no two processes compile into the same build directory
     if rank == 0:
-        peak, peak_kind = measured_peaks()
-        out_bytes = sum(v.numel() * v.element_size() for v in out.values())
-        per_launch_s = sec / args.steps / 1.0
-        achieved = out_bytes / per_launch_s / 1e9
-        traffic = (wl['dram_bytes_per_traj'] * n
+        _build.build()
+    if world > 1:
+        dist.barrier()
+    peaks = measure_pipe_peaks(dev)
+    head = plain_record(args.workload, wl, args, dev, peaks, args.steps,
+                        args.warmup, world, rank)
+    line = None
+    if rank == 0:
+        hbm, hbm_kind = measured_peaks()
+        per_launch_s = head['ms_per_step'] / 1e3
+        achieved = head['out_bytes'] / per_launch_s / 1e9
+        traffic = (wl['dram_bytes_per_traj'] * wl['n']
                    if 'dram_bytes_per_traj' in wl else None)
-        issue = None
-        if 'warp_inst_per_event' in wl and clocks.get('sm_mhz'):
-            # instruction-issue roofline: warp instructions per second
-            # against 4 schedulers per SM at the sampled SM clock
-            sms = torch.cuda.get_device_properties(dev).multi_processor_count
-            a = value / world * wl['warp_inst_per_event'] / 1e12
-            pk = sms * 4 * clocks['sm_mhz'] * 1e6 / 1e12
-            issue = {'bound': 'issue', 'achieved': a, 'peak': pk,
-                     'unit': 'T warp-inst/s', 'frac': a / pk,
-                     'warp_inst_per_event': wl['warp_inst_per_event'],
-                     'source': 'ncu instruction count per event x measured '
-                               'events/s; peak 4 issue slots/SM/cycle'}
+        roof = head.get('roofline') or {}
+        roof['traffic'] = traffic
+        roof['hbm'] = {'bound': 'hbm', 'achieved': achieved, 'peak': hbm,
+                       'unit': 'GB/s', 'frac': achieved / hbm,
+                       'peak_source': hbm_kind,
+                       'algorithmic_bytes': head['out_bytes'],
+                       'traffic': traffic,
+                       'note': 'HBM carries only the sample output; '
+                               'traffic from an ncu capture of 229376 '
+                               'trajectories scaled by trajectories'}
+        if 'warp_inst_per_event' in wl and (head['clocks'] or {}).get(
+                'sm_mhz'):
+            sms = torch.cuda.get_device_properties(
+                dev).multi_processor_count
+            a = head['value'] / world * wl['warp_inst_per_event'] / 1e12
+            pk = sms * 4 * head['clocks']['sm_mhz'] * 1e6 / 1e12
+            roof['executed_issue'] = {
+                'achieved': a, 'peak': pk, 'unit': 'T warp-inst/s',
+                'frac': a / pk,
+                'warp_inst_per_event': wl['warp_inst_per_event'],
+                'source': 'ncu executed-instruction count per event x '
+                          'measured events/s; peak 4 issue slots/SM/cycle '
+                          'at the sampled clock'}
         line = {
-            'metric': METRIC, 'value': value, 'unit': UNIT,
+            'metric': METRIC, 'value': head['value'], 'unit': UNIT,
             'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
-            'ms_per_step': total_ms / args.steps, 'higher_is_better': True,
+            'ms_per_step': head['ms_per_step'], 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32/f64',
             'data': 'synthetic',
-            'config': {'workload': wl['desc'], 'trajectories_per_gpu': n,
+            'config': {'workload': wl['desc'],
+                       'trajectories_per_gpu': wl['n'],
                        'l2': 'flushed (256 MiB write) before every step',
                        'parallelism': 'trajectory shards, one per GPU'},
-            'trajectories_per_s': n * world * args.steps / sec,
-            'events_per_step': events / args.steps,
-            'error_trajectories': int(errs),
-            # this library's kernels in the timed region: the simulation,
-            # plus the two-kernel score reduction of the gradient form
-            'gpu_launches': args.steps * (3 if grad else 1),
-            'e2e': {'value': e2e_value, 'unit': UNIT,
-                    'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h},
-            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak,
-                         'unit': 'GB/s', 'frac': achieved / peak,
-                         'traffic': traffic, 'peak_source': peak_kind,
-                         'algorithmic_bytes': out_bytes,
-                         'note': 'the kernel is CUDA-core issue bound; HBM '
-                                 'carries only the sample output (traffic: '
-                                 'partially written 32-byte sectors of the '
-                                 '[kappa][ita][U] layout, scaled from a '
-                                 '229376-trajectory ncu capture)'},
-            'issue': issue,
-            'clocks': clocks,
+            'trajectories_per_s': head['trajectories_per_s'],
+            'events_per_step': head['events_per_step'],
+            'error_trajectories': head['error_trajectories'],
+            'status_counts': head['status_counts'],
+            'gpu_launches': head['gpu_launches'],
+            'e2e': head['e2e'], 'roofline': roof,
+            'clocks': head['clocks'], 'pipe_peaks': peaks,
         }
-        if not args.no_cpu_baseline and world == 1:
-            line['cpu_baseline'] = cpu_baseline(wl)
-        if not args.no_forms and world == 1:
-            line['forms'] = batch_vs_plain('sweep', dev, full=False)
+        if 'cpu_baseline' in head:
+            line['cpu_baseline'] = head['cpu_baseline']
+    if world == 1 and not args.no_configs:
+        line['configs'] = other_configs(args, dev, peaks)
+    if rank == 0:
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def other_configs(args, dev, peaks):
+    """The other configurations of the metric, each as its own record:
+    Lotka-Volterra direct method (1024 trajectories), the telegraph
+    gradient (1M trajectories, forward + backward), the 16384-set sweep
+    and the 4096 synthetic networks (batched, with the plain
+    one-launch-per-model form on a subset of the same models)."""
+    import torch
+    wls = workloads()
+    steps = max(1, min(args.steps, 5))
+    out = {}
+    for name in ('lv_ssa', 'telegraph_grad'):
+        out[name] = plain_record(name, wls[name], args, dev, peaks, steps, 2)
+        torch.cuda.empty_cache()
+    out['sweep'] = batch_vs_plain('sweep', dev, subset=FORMS['sweep'][0],
+                                  budget=FORMS['sweep'][1])
+    out['synthetic'] = batch_vs_plain('synthetic', dev,
+                                      subset=FORMS['synthetic'][0],
+                                      budget=FORMS['synthetic'][1])
+    return out
+
+
+# (plain-form subset size, step budget) of the batched configurations.
+# The sweep runs every trajectory to t_end (or int32 overflow) within 2e6
+# steps; the synthetic networks include explosive ones that no budget
+# finishes (10x the budget: 6x the time, 3% more completed firings), so
+# they keep 20,000 steps and report the unfinished fraction.
+FORMS = {'sweep': (64, 2_000_000), 'synthetic': (32, 20_000)}
 
 
 def forms_main(args):
@@ -596,7 +839,9 @@ def forms_main(args):
     dev = torch.device('cuda', int(os.environ.get('LOCAL_RANK', '0')))
     torch.cuda.set_device(dev)
     _build.build()
-    r = batch_vs_plain(args.workload, dev, steps=args.steps, full=True)
+    subset, budget = FORMS[args.workload]
+    r = batch_vs_plain(args.workload, dev, subset=subset, steps=args.steps,
+                       full=True, budget=budget)
     full = r['batched_full']
     line = {'metric': METRIC, 'value': full['completed_events_per_s'],
             'all_events_per_s': full['events_per_s'], 'unit': UNIT,

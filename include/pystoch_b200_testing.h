@@ -33,6 +33,15 @@ int pyst_test_math(const double* d_x, int64_t n, int which, double* d_out,
 int pyst_test_poisson(const float* d_lam, int64_t n, uint64_t seed,
                       int32_t* d_out, void* stream);
 
+/* Issue-rate probe of one arithmetic pipe (the denominators of the
+ * instruction roofline): `blocks` blocks of 256 threads each run `iters`
+ * iterations of 8 independent chains of one operation -- which 0 FP32
+ * fma, 1 INT32 multiply-add, 2 FP64 fma, 3 INT32 xor + add (two ALU
+ * operations) -- and write one double per thread to d_sink.  The caller
+ * times it: 8 * iters * 256 * blocks chain steps. */
+int pyst_test_pipe(int32_t which, int32_t iters, int32_t blocks,
+                   double* d_sink, void* stream);
+
 /* Bound of the model-staging wait of every later run call in this process
  * (polls of the staging mbarrier; PYST_MBAR_POLL_LIMIT by default).  With
  * 0 every staging wait gives up at once, so a test can see the timeout

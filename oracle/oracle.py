@@ -220,7 +220,9 @@ def simulate(model, n_traj, method, seed=0, traj_id_base=0, warp=False,
         'seqhash': np.zeros(n_traj, dtype=np.uint64),
         't_final': np.zeros(n_traj, dtype=np.float64),
         'score': np.zeros((n_traj, R), dtype=np.float64),
-        'steps': np.zeros((n_traj, 2), dtype=np.int64),
+        # SSA steps, leaps, inversion Poisson draws and their search
+        # iterations, PTRS draws and their iterations
+        'steps': np.zeros((n_traj, 6), dtype=np.int64),
     }
     oo = _OOut(res['samples'].ctypes.data, n_traj,
                res['status'].ctypes.data, res['events'].ctypes.data,

@@ -191,11 +191,14 @@ static void pblock(const opkey* pk, uint32_t blk, uint32_t w[4]) {
   oracle_philox(ctr, key, w);
 }
 
-int oracle_poisson(float lam, const opkey* pk) {
+/* cnt (optional): [0] inversion draws, [1] inversion search iterations,
+ * [2] PTRS draws, [3] PTRS iterations. */
+static int oracle_poisson_counted(float lam, const opkey* pk, int64_t* cnt) {
   if (!(lam > 0.0f)) return 0;
   if (!(lam <= 1.0e9f)) return -2;
   uint32_t w[4];
   if (lam < 10.0f) {
+    if (cnt) cnt[0]++;
     pblock(pk, 0u, w);
     double u = u32co(w[0]);
     double l = (double)lam;
@@ -204,6 +207,7 @@ int oracle_poisson(float lam, const opkey* pk) {
     int k = 0;
     while (u > F && k < 200) {
       k++;
+      if (cnt) cnt[1]++;
       double inv = 1.0 / (double)k;
       p = (p * l) * inv;
       F = F + p;
@@ -217,8 +221,10 @@ int oracle_poisson(float lam, const opkey* pk) {
   float invalpha = 1.1239f + 1.1328f / (b - 3.4f);
   float vr = 0.9277f - 3.6224f / (b - 2.0f);
   double log_invalpha = oracle_log((double)invalpha);
+  if (cnt) cnt[2]++;
   for (int it = 0; it < 64; ++it) {
     uint32_t wu, wv;
+    if (cnt) cnt[3]++;
     if ((it & 1) == 0) {
       pblock(pk, (uint32_t)(it >> 1), w);
       wu = w[0];
@@ -247,6 +253,10 @@ int oracle_poisson(float lam, const opkey* pk) {
     if (lhs <= rhs) return (int)kf;
   }
   return -1;
+}
+
+int oracle_poisson(float lam, const opkey* pk) {
+  return oracle_poisson_counted(lam, pk, NULL);
 }
 
 /* ------------------------------------------------------------- model */
@@ -289,7 +299,9 @@ typedef struct {
   uint64_t* seqhash;
   double* t_final;
   double* score; /* [n][R] */
-  int64_t* steps; /* [n][2]: SSA steps, leaps (optional) */
+  int64_t* steps; /* [n][6] (optional): SSA steps, leaps, inversion Poisson
+                     draws, their search iterations, PTRS draws, their
+                     iterations */
 } oout;
 
 #define FNV_OFF 0xcbf29ce484222325ull
@@ -502,6 +514,7 @@ static void one_trajectory(const omodel* m, const float* rate32,
   double t = 0.0;
   int f = 0;
   int64_t events = 0, steps = 0, n_ssa = 0, n_leap = 0;
+  int64_t pcnt[4] = {0, 0, 0, 0};
   uint64_t h = FNV_OFF;
   int status = 0, fill_state = 0;
   int64_t budget = ru->step_budget ? ru->step_budget : (1ll << 62);
@@ -594,7 +607,7 @@ static void one_trajectory(const omodel* m, const float* rate32,
                           0x80000000u | ((uint32_t)j << 12) |
                               ((uint32_t)retry << 6),
                           rs.c2, rs.c3};
-              int k = oracle_poisson(lam, &pk);
+              int k = oracle_poisson_counted(lam, &pk, pcnt);
               if (k < 0) bad = 1;
               K[j] = k < 0 ? 0 : k;
             }
@@ -709,8 +722,9 @@ static void one_trajectory(const omodel* m, const float* rate32,
   if (o->seqhash) o->seqhash[u] = h;
   if (o->t_final) o->t_final[u] = t;
   if (o->steps) {
-    o->steps[2 * u] = n_ssa;
-    o->steps[2 * u + 1] = n_leap;
+    o->steps[6 * u] = n_ssa;
+    o->steps[6 * u + 1] = n_leap;
+    for (int q = 0; q < 4; ++q) o->steps[6 * u + 2 + q] = pcnt[q];
   }
   if (o->score)
     for (int j = 0; j < R; ++j) o->score[u * R + j] = cnt[j] - integ[j];

@@ -165,6 +165,48 @@ __global__ void k_poisson(const float* lam, int64_t n, uint64_t seed,
   out[i] = poisson(lam[i], leap_key(s, 7u, (int)(i & 1023), 3));
 }
 
+// Issue-rate probe of one arithmetic pipe: 8 independent dependency chains
+// per thread, so the pipe, not latency, bounds it.  OP 0: FP32 fused
+// multiply-add; 1: INT32 multiply-add (mad.lo.u32); 2: FP64 fused
+// multiply-add; 3: INT32 xor-shift-add (the ALU forms Philox's xors and
+// key additions use).  One operation per chain per iteration.
+template <int OP>
+__global__ void __launch_bounds__(256) k_pipe(int iters, double* sink) {
+  const uint32_t t = blockIdx.x * 256u + threadIdx.x;
+  float f[8];
+  uint32_t x[8];
+  double d[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    f[c] = (float)(t + c) * 1e-3f;
+    x[c] = t * 8u + (uint32_t)c;
+    d[c] = (double)(t + c) * 1e-3;
+  }
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      if (OP == 0) f[c] = __fmaf_rn(f[c], 0.99999f, 1e-7f);
+      // (integer chains in inline PTX: the compiler may not fold two
+      // steps of a multiply-add chain into one)
+      if (OP == 1)
+        asm volatile("mad.lo.u32 %0, %0, %1, %2;"
+                     : "+r"(x[c])
+                     : "r"(0x9E3779B1u), "r"(0x7F4A7C15u));
+      if (OP == 2) d[c] = __fma_rn(d[c], 0.99999, 1e-9);
+      if (OP == 3)
+        asm volatile("xor.b32 %0, %0, %1;\n\tadd.u32 %0, %0, %2;"
+                     : "+r"(x[c])
+                     : "r"((uint32_t)i), "r"(0x7F4A7C15u));
+    }
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int c = 0; c < 8; ++c)
+    acc = __dadd_rn(acc, OP == 0 ? (double)f[c]
+                         : OP == 2 ? d[c] : (double)x[c]);
+  sink[t] = acc;
+}
+
 }  // namespace
 
 int64_t score_backward_blocks(int64_t U) {
@@ -280,6 +322,18 @@ int pyst_score_backward_noalloc(const int32_t* samples, const double* score,
   return launch_score_backward(samples, score, n_traj, kappa, ita,
                                n_reactions, mean, var, gmean, gvar, part,
                                d_grad, (cudaStream_t)stream);
+}
+
+int pyst_test_pipe(int32_t which, int32_t iters, int32_t blocks,
+                   double* d_sink, void* stream) {
+  if (!d_sink || iters < 1 || blocks < 1 || which < 0 || which > 3)
+    return PYST_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (which == 0) k_pipe<0><<<blocks, 256, 0, st>>>(iters, d_sink);
+  if (which == 1) k_pipe<1><<<blocks, 256, 0, st>>>(iters, d_sink);
+  if (which == 2) k_pipe<2><<<blocks, 256, 0, st>>>(iters, d_sink);
+  if (which == 3) k_pipe<3><<<blocks, 256, 0, st>>>(iters, d_sink);
+  return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
 }
 
 int pyst_test_philox(uint64_t seed, uint64_t id, uint64_t n0, int64_t count,

@@ -94,8 +94,320 @@ __global__ void __launch_bounds__(128, PYST_THREAD_MINB)
 #define PYST_GROUP_LANES 32
 #endif
 constexpr int kGroupLanes = PYST_GROUP_LANES;
+// 0 keeps the lane groups on the plain lockstep loop (no lane tree)
+#ifndef PYST_SPEC_TREE
+#define PYST_SPEC_TREE 1
+#endif
 // runs of at most this many trajectories per SM take the lane groups
 constexpr int kGroupMaxPerSm = 16;
+
+// ---------------------------------------------------------------------
+// Speculative lane tree (the lane groups' fast path for small mass-action
+// models).  A step's selection j depends on the state, which depends on the
+// previous selection: one dependent chain per trajectory.  Here the 32
+// lanes of the trajectory's warp evaluate the next D steps at once: the
+// lane at depth d with path (j_1 .. j_d) takes the state after firing
+// j_1 .. j_d, computes its propensities, total, tau and selection for step
+// d + 1 (with step d + 1's random numbers), and a few ballots publish every
+// lane's selection, so each lane walks the tree from the root along the
+// selections to the true path.  Lanes per depth grow as R^d; D is the
+// largest depth with 1 + R + ... + R^(D-1) <= 32 (at most kSpecMaxDepth):
+// Lotka-Volterra (R = 3) advances 3 steps per pass on 13 lanes.
+// The passes commit only when none of the D steps reaches a sample time,
+// absorbs, runs out of step budget or leaves the int32 range; otherwise D
+// exact single steps run instead (thread_round's order of operations, which
+// handles every such case).  Every lane does exactly the arithmetic of the
+// step it evaluates, so results are those of one thread per trajectory,
+// bit for bit.  Species counts (at most MAXS) live in registers, read and
+// written by unrolled selects.
+constexpr int kSpecMaxDepth = 5;
+
+template <int MAXS>
+__device__ __forceinline__ int reg_get(const int (&x)[MAXS], int sp) {
+  int v = x[0];
+#pragma unroll
+  for (int s = 1; s < MAXS; ++s) v = (sp == s) ? x[s] : v;
+  return v;
+}
+
+// x += the packed net change d, entry by entry with the range check of
+// thread_round (an entry that would leave [0, 2^31) is skipped and flags
+// the step); false if any entry was out of range.
+template <int MAXS>
+__device__ __forceinline__ bool reg_apply(int (&x)[MAXS], uint32_t d) {
+  bool ok = true;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    if (q < pnet_count(d)) {
+      const int sp = pnet_species(d, q);
+      const int64_t nx = (int64_t)reg_get(x, sp) + pnet_delta(d, q);
+      if (nx < 0 || nx > PYST_I32MAX) {
+        ok = false;
+      } else {
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s)
+          if (s == sp) x[s] = (int)nx;
+      }
+    }
+  }
+  return ok;
+}
+
+// Propensities (FP32, packed descriptors), their FP64 total, and the
+// direct-method selection for uniform-times-total r, as thread_round.
+template <int MAXR, int MAXS>
+__device__ __forceinline__ double reg_propensities(const ModelView& m,
+                                                   const int (&x)[MAXS],
+                                                   float (&a)[MAXR]) {
+  double a0 = 0.0;
+  auto xget = [&](int i) { return reg_get(x, i); };
+#pragma unroll
+  for (int j = 0; j < MAXR; ++j) {
+    if (j >= m.R) break;
+    a[j] = propensity_packed(m.rate(j), m.pk[j], xget);
+    a0 = __dadd_rn(a0, (double)a[j]);
+  }
+  return a0;
+}
+
+template <int MAXR>
+__device__ __forceinline__ int select_reaction(const float (&a)[MAXR], int R,
+                                               double r) {
+  double cum = 0.0;
+  int lastnz = -1, sel = -1;
+#pragma unroll
+  for (int j = 0; j < MAXR; ++j) {
+    if (j >= R) break;
+    cum = __dadd_rn(cum, (double)a[j]);
+    if (a[j] > 0.0f) lastnz = j;
+    if (cum >= r) {
+      sel = j;
+      break;
+    }
+  }
+  return sel < 0 ? lastnz : sel;
+}
+
+// Exponential variate and uniform of main-stream block `blk`.
+__device__ __forceinline__ void step_variates(Stream& rs, uint64_t blk,
+                                              double& e, double& u) {
+  rs.n = blk;
+  const uint4 w = next_block(rs);
+  e = -pyst_log(u53(w.x, w.y));
+  u = u53(w.z, w.w);
+}
+
+// One whole trajectory by the calling warp (all 32 lanes; lane 0 writes).
+template <int MAXR, int MAXS>
+__device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
+                              uint64_t traj_id, const TrajOut& o) {
+  const int R = m.R, S = m.S, ita = m.ita, kappa = m.kappa;
+  const int lane = threadIdx.x & 31;
+  // tree shape: D levels, lanes [start_d, start_d + R^d) at depth d
+  int D = 1, used = 1, width = 1;
+  while (D < kSpecMaxDepth && used + width * R <= 32) {
+    width *= R;
+    used += width;
+    ++D;
+  }
+  int dl = 0, il = 0;
+  {
+    int st = 0, w = 1;
+    for (int d = 0; d < D; ++d) {
+      if (lane >= st && lane < st + w) {
+        dl = d;
+        il = lane - st;
+      }
+      st += w;
+      w *= R;
+    }
+  }
+  // this lane's path j_1 .. j_dl: base-R digits of il, first firing first
+  int path[kSpecMaxDepth];
+  {
+    int v = il;
+#pragma unroll
+    for (int k = kSpecMaxDepth - 1; k >= 0; --k) {
+      if (k < dl) {
+        path[k] = v % R;
+        v /= R;
+      } else {
+        path[k] = 0;
+      }
+    }
+  }
+  const bool in_tree = lane < used;
+
+  Stream rs = make_stream(ra.seed, traj_id);
+  int x[MAXS];
+#pragma unroll
+  for (int s = 0; s < MAXS; ++s) x[s] = s < S ? m.x0(s) : 0;
+  // step variates: lane g holds blocks vb + g (cur) and vb + 32 + g (nxt)
+  uint64_t vb = 0;
+  double e_c, u_c, e_n, u_n;
+  step_variates(rs, (uint64_t)lane, e_c, u_c);
+  step_variates(rs, 32u + (uint64_t)lane, e_n, u_n);
+  auto variate = [&](int64_t step, double& e, double& u) {
+    const int off = (int)(step - (int64_t)vb);  // 0 <= off < 64
+    const int own = off & 31;
+    const double ec = __shfl_sync(0xffffffffu, e_c, own);
+    const double en = __shfl_sync(0xffffffffu, e_n, own);
+    const double uc = __shfl_sync(0xffffffffu, u_c, own);
+    const double un = __shfl_sync(0xffffffffu, u_n, own);
+    e = off >= 32 ? en : ec;
+    u = off >= 32 ? un : uc;
+  };
+
+  double t = 0.0;
+  int f = 0;
+  double tf = m.time(0);
+  int64_t steps = 0, events = 0;
+  uint64_t h = PYST_FNV_OFFSET;
+  int status = PYST_TRAJ_DONE;
+  bool fill_state = false, done = false;
+  const int64_t budget = ra.step_budget;
+  constexpr int kSelBits = MAXR <= 2 ? 1 : (MAXR <= 4 ? 2 : 3);
+
+  while (!done) {
+    if (steps - (int64_t)vb >= 32) {
+      vb += 32;
+      e_c = e_n;
+      u_c = u_n;
+      step_variates(rs, vb + 32u + (uint64_t)lane, e_n, u_n);
+    }
+    bool committed = false;
+    if (D > 1) {
+      // ---- every lane: the step at the end of its path --------------
+      int xs[MAXS];
+#pragma unroll
+      for (int s = 0; s < MAXS; ++s) xs[s] = x[s];
+      bool ok = in_tree;
+#pragma unroll
+      for (int k = 0; k < kSpecMaxDepth; ++k)
+        if (k < dl) ok &= reg_apply(xs, m.pk[R + path[k]]);
+      float a[MAXR];
+      const double a0 = reg_propensities<MAXR>(m, xs, a);
+      double e, u;
+      variate(steps + dl, e, u);
+      const double tau = __ddiv_rn(e, a0);
+      const int sel = select_reaction<MAXR>(a, R, __dmul_rn(u, a0));
+      ok &= a0 != 0.0;
+      unsigned sb[kSelBits];
+#pragma unroll
+      for (int b = 0; b < kSelBits; ++b)
+        sb[b] = __ballot_sync(0xffffffffu, (sel >> b) & 1);
+      const unsigned bad = __ballot_sync(0xffffffffu, !ok);
+      // ---- walk the tree along the selections (uniform) ---------------
+      int J[kSpecMaxDepth], L[kSpecMaxDepth];
+      bool walk = true;
+      {
+        int i = 0, st = 0, w = 1;
+#pragma unroll
+        for (int d = 0; d < kSpecMaxDepth; ++d) {
+          if (d < D && walk) {
+            const int ln = st + i;
+            if ((bad >> ln) & 1u) walk = false;
+            int j = 0;
+#pragma unroll
+            for (int b = 0; b < kSelBits; ++b) j |= (int)((sb[b] >> ln) & 1u) << b;
+            J[d] = j;
+            L[d] = ln;
+            i = i * R + j;
+            st += w;
+            w *= R;
+          } else {
+            J[d] = 0;
+            L[d] = 0;
+          }
+        }
+      }
+      if (walk && steps + D <= budget) {
+        double tt = t;
+#pragma unroll
+        for (int d = 0; d < kSpecMaxDepth; ++d) {
+          const double td = __shfl_sync(0xffffffffu, tau, L[d]);
+          if (d < D) tt = __dadd_rn(tt, td);
+        }
+        if (tt < tf) {
+          int xn[MAXS];
+#pragma unroll
+          for (int s = 0; s < MAXS; ++s) xn[s] = x[s];
+          bool inr = true;
+#pragma unroll
+          for (int d = 0; d < kSpecMaxDepth; ++d)
+            if (d < D) inr &= reg_apply(xn, m.pk[R + J[d]]);
+          if (inr) {
+#pragma unroll
+            for (int s = 0; s < MAXS; ++s) x[s] = xn[s];
+#pragma unroll
+            for (int d = 0; d < kSpecMaxDepth; ++d)
+              if (d < D) h = seq_mix(h, (uint64_t)J[d]);
+            t = tt;
+            steps += D;
+            events += D;
+            committed = true;
+          }
+        }
+      }
+    }
+    if (committed) continue;
+    // ---- D exact single steps ------------------------------------------
+    for (int q = 0; q < D && !done; ++q) {
+      float a[MAXR];
+      const double a0 = reg_propensities<MAXR>(m, x, a);
+      if (a0 == 0.0) {
+        status = PYST_TRAJ_ABSORBED;
+        fill_state = true;
+        done = true;
+        break;
+      }
+      if (steps >= budget) {
+        status = PYST_TRAJ_STEP_BUDGET;
+        done = true;
+        break;
+      }
+      double e, u;
+      variate(steps, e, u);
+      steps++;
+      const double tau = __ddiv_rn(e, a0);
+      const int sel = select_reaction<MAXR>(a, R, __dmul_rn(u, a0));
+      const double tn = __dadd_rn(t, tau);
+      while (tn >= tf) {
+        if (lane == 0)
+          for (int k = 0; k < kappa; ++k)
+            store_sample(o, ita, k, f, reg_get(x, m.out(k)));
+        f++;
+        if (f == ita) {
+          done = true;
+          break;
+        }
+        tf = m.time(f);
+      }
+      t = tn;
+      if (done) break;
+      if (!reg_apply(x, m.pk[R + sel])) {
+        status = PYST_TRAJ_OVERFLOW;
+        done = true;
+        break;
+      }
+      events++;
+      h = seq_mix(h, (uint64_t)sel);
+    }
+  }
+  if (lane == 0) {
+    for (; f < ita; ++f)
+      for (int k = 0; k < kappa; ++k)
+        store_sample(o, ita, k, f,
+                     fill_state ? reg_get(x, m.out(k)) : -1);
+    if (o.status) *o.status = (uint8_t)status;
+    if (o.events) *o.events = events;
+    if (o.seqhash) *o.seqhash = h;
+    if (o.t_final) *o.t_final = t;
+  }
+}
+
+// species held in registers by the lane tree
+constexpr int kSpecMaxSpecies = 8;
 
 template <int MAXR, int LG>
 __global__ void __launch_bounds__(128)
@@ -130,9 +442,16 @@ __global__ void __launch_bounds__(128)
   m.fast = __syncthreads_and(pack_reactions(m, pk)) != 0;
   int32_t* xcol = xbase + threadIdx.x;
   int64_t* slot = (int64_t*)(xbase + (size_t)m.S * bs) + threadIdx.x;
+  // the lane tree needs a whole warp, packed reactions and few species
+  const bool tree = LG == 32 && m.fast && m.S <= kSpecMaxSpecies &&
+                    PYST_SPEC_TREE;
   for (; u < n_traj; u += ngroups) {
     const TrajOut o = ob.at(0, u, 0, 0, ob.stride, m.R);
     const uint64_t id = id_base + (uint64_t)u;
+    if (tree) {
+      run_spec_tree<MAXR, kSpecMaxSpecies>(m, ra, id, o);
+      continue;
+    }
     TState st;
     thread_init<false>(m, xcol, bs, st);
     double integ[1] = {0.0};
