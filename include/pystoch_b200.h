@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define PYST_ABI_VERSION 2
+#define PYST_ABI_VERSION 3
 
 /* ---- return codes ------------------------------------------------------ */
 enum {
@@ -135,6 +135,14 @@ typedef struct pyst_run_desc {
   int64_t step_budget;         /* max steps per trajectory (0 = 2^62)       */
   int32_t block_size;          /* 0 = library default                       */
   int32_t flags;               /* PYST_FLAG_* bits                          */
+  /* Geometry of the mode-sorted tau-leaping kernel (thread mapping); 0
+   * takes the default.  Results do not depend on it, only the speed. */
+  int32_t round_ssa;           /* SSA steps per scheduling round (32)       */
+  int32_t round_leap;          /* leaps per scheduling round (3)            */
+  int32_t pool_slots;          /* trajectory slots per thread: 1 or 2 (2)   */
+  int32_t sorted_block;        /* threads per block: 64..896, a multiple of
+                                  32 (896; smaller when the pools do not fit
+                                  shared memory)                            */
 } pyst_run_desc;
 
 /* Outputs (device pointers).  `samples` is required, the rest optional. */
@@ -198,19 +206,30 @@ int pyst_tau_leap_run(const uint32_t* h_blob, const uint32_t* d_blob,
 /* ---- batched persistent runs -------------------------------------------- */
 
 /* One work item: a model, its trajectories and where its outputs go.
- * Offsets are in elements of the corresponding output arrays; an item's
- * samples are [kappa][ita][n_traj] starting at sample_offset. */
+ * Offsets are in elements of the corresponding output arrays; a model's
+ * samples are [kappa][ita][U] starting at sample_offset, U its trajectory
+ * count.  A model may be split into chunks (consecutive items with the
+ * same offsets): chunk c runs the model's trajectories chunk_begin ..
+ * chunk_begin + n_traj - 1 of U = model_n_traj, so several blocks share a
+ * large model; the block that finishes the model's last chunk computes its
+ * statistics.  An unsplit model has chunk_begin 0 and model_n_traj 0. */
 typedef struct pyst_batch_item {
   int64_t blob_offset;     /* word offset of the model blob in d_blobs     */
   int64_t n_traj;          /* trajectories of this item                    */
-  int64_t traj_id_base;    /* Philox id of its trajectory 0                */
-  int64_t sample_offset;   /* element offset of its [kappa][ita][n_traj]   */
+  int64_t traj_id_base;    /* Philox id of the model's trajectory 0        */
+  int64_t sample_offset;   /* element offset of the model's [kappa][ita][U]*/
   int64_t traj_offset;     /* element offset into status/events/... arrays */
-  int64_t score_offset;    /* element offset into score ([n_traj][R])      */
+  int64_t score_offset;    /* element offset into score ([U][R])           */
   int64_t stats_offset;    /* element offset into stats                    */
   int64_t jac_offset;      /* element offset into jacobian                 */
   int32_t method;          /* PYST_METHOD_*                                */
   int32_t mapping;         /* PYST_MAP_THREAD or PYST_MAP_WARP             */
+  int64_t chunk_begin;     /* first trajectory of this chunk in its model  */
+  int64_t model_n_traj;    /* U of a split model (0: unsplit, U = n_traj)  */
+  int32_t group;           /* split model: its completion counter,
+                              0 <= group < n_items, one per model           */
+  int32_t group_chunks;    /* split model: its number of chunks (0 or 1:
+                              unsplit)                                      */
 } pyst_batch_item;
 
 /* Largest model of a batch (sizes the shared-memory layout). */
@@ -221,7 +240,8 @@ typedef struct pyst_batch_limits {
   int32_t reserved;
 } pyst_batch_limits;
 
-/* Workspace bytes pyst_batch_run needs for n_items items. */
+/* Workspace bytes pyst_batch_run needs for n_items items: the work-queue
+ * counter and one completion counter per item (split models). */
 int pyst_batch_workspace_size(int64_t n_items, size_t* bytes);
 
 /* Run every item in one persistent launch.  `d_items` is device memory

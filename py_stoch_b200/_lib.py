@@ -41,6 +41,7 @@ MAX_REACTIONS = 4096
 THREAD_MAX_REACTIONS = 32
 MAX_BLOB_WORDS = 12288
 RUN_WORKSPACE_BYTES = 256
+ABI_VERSION = 3
 NOALLOC_SCRATCH_BYTES = 1 << 20
 SCORE_CHUNK = 256
 SUMS_MAX_TRAJ = 2**31 - 1
@@ -69,7 +70,9 @@ class RunDesc(C.Structure):
                 ('seed', C.c_uint64), ('method', C.c_int32),
                 ('mapping', C.c_int32), ('ssa_fallback_steps', C.c_int32),
                 ('max_leap_retries', C.c_int32), ('step_budget', C.c_int64),
-                ('block_size', C.c_int32), ('flags', C.c_int32)]
+                ('block_size', C.c_int32), ('flags', C.c_int32),
+                ('round_ssa', C.c_int32), ('round_leap', C.c_int32),
+                ('pool_slots', C.c_int32), ('sorted_block', C.c_int32)]
 
 
 class Outputs(C.Structure):
@@ -83,7 +86,9 @@ class BatchItem(C.Structure):
                 ('traj_id_base', C.c_int64), ('sample_offset', C.c_int64),
                 ('traj_offset', C.c_int64), ('score_offset', C.c_int64),
                 ('stats_offset', C.c_int64), ('jac_offset', C.c_int64),
-                ('method', C.c_int32), ('mapping', C.c_int32)]
+                ('method', C.c_int32), ('mapping', C.c_int32),
+                ('chunk_begin', C.c_int64), ('model_n_traj', C.c_int64),
+                ('group', C.c_int32), ('group_chunks', C.c_int32)]
 
 
 class BatchLimits(C.Structure):

@@ -1,5 +1,8 @@
-"""Autotuner for batched runs: thread- vs warp-per-trajectory mapping per
-model bucket, and the batch block size, chosen by measurement.
+"""Autotuner: thread- vs warp-per-trajectory mapping per model bucket and
+the batch block size for batched runs, and the mode-sorted tau-leaping
+scheduler's geometry (round lengths, trajectory slots per thread, block
+size, which set its shared-memory layout) for single-model runs, chosen by
+measurement.
 
 Buckets are (method, reaction-count bucket, species-count bucket).  For
 each bucket present in a batch the tuner builds a small trial batch from up
@@ -25,6 +28,14 @@ from .simulator import _method, _torch
 
 R_EDGES = (8, 32, 64, 128, 256, 1024, 4096)
 S_EDGES = (16, 64, 1024)
+N_EDGES = (4096, 65536, 1 << 20, 1 << 40)
+
+# Candidate geometries of the mode-sorted scheduler: (SSA steps, leaps) per
+# round x slots per thread x block size.  Every one gives the same results
+# (the schedule never changes a trajectory's arithmetic).
+ROUNDS = ((16, 2), (32, 3), (64, 4))
+POOLS = (1, 2)
+SORTED_BLOCKS = (896, 448)
 
 _lock = threading.Lock()
 
@@ -148,6 +159,61 @@ class Autotuner(object):
         self.table[key] = {'block': best, 'events_per_s': res}
         self._save()
         return best
+
+    def _time_single(self, model, n_traj, method, geometry, reps=2):
+        from .simulator import simulate
+        torch = _torch()
+        stream = torch.cuda.current_stream(self.device)
+        out = {}
+        best = 0.0
+        for r in range(reps + 1):
+            st = torch.cuda.Event(enable_timing=True)
+            en = torch.cuda.Event(enable_timing=True)
+            st.record(stream)
+            res = simulate(model, n_traj, method=method, seed=0x5EED + r,
+                           device=self.device, stream=stream, out=out,
+                           geometry=geometry)
+            en.record(stream)
+            en.synchronize()
+            out = {k: v for k, v in res.items() if k != '_keepalive'}
+            if r:  # the first run is a warm-up
+                ev = float(res['events'].sum().item())
+                best = max(best, ev / max(st.elapsed_time(en), 1e-3) * 1e3)
+        return best
+
+    def tune_geometry(self, model, n_traj, method='tau', force=False):
+        """Measure every candidate geometry of the mode-sorted scheduler on
+        ``n_traj`` trajectories of ``model`` (whole runs, events per second
+        by CUDA events, best of two after a warm-up) and cache the fastest
+        for the model's bucket and run size.  Returns the geometry dict
+        (keyword ``geometry`` of :func:`py_stoch_b200.simulator.simulate`).
+        """
+        key = 'geom/%s/N%d' % (bucket(model, method),
+                               _edge(int(n_traj), N_EDGES))
+        if key in self.table and not force:
+            return dict(self.table[key]['geometry'])
+        res = {}
+        for (rs, rl) in ROUNDS:
+            for pool in POOLS:
+                for blk in SORTED_BLOCKS:
+                    g = {'round_ssa': rs, 'round_leap': rl,
+                         'pool_slots': pool, 'sorted_block': blk}
+                    name = '%d/%d/p%d/b%d' % (rs, rl, pool, blk)
+                    res[name] = (g, self._time_single(model, n_traj, method,
+                                                      g))
+        best = max(res, key=lambda k: res[k][1])
+        self.table[key] = {'geometry': res[best][0],
+                           'events_per_s': {k: v[1] for k, v in
+                                            res.items()}}
+        self.timings[key] = self.table[key]['events_per_s']
+        self._save()
+        return dict(res[best][0])
+
+    def geometry(self, model, n_traj, method='tau'):
+        """Cached geometry for this model bucket and run size, or None."""
+        ent = self.table.get('geom/%s/N%d' % (bucket(model, method),
+                                              _edge(int(n_traj), N_EDGES)))
+        return dict(ent['geometry']) if ent else None
 
     # ---- lookup ----------------------------------------------------------
     def mapping(self, model, method):

@@ -54,7 +54,7 @@ class Batch(object):
     def __init__(self, models, n_traj, method='direct', mapping='auto',
                  traj_id_base=None, device=None, score=False, status=True,
                  events=True, seqhash=False, t_final=False, order='cost',
-                 mapping_fn=None, stats=False, jacobian=False):
+                 mapping_fn=None, stats=False, jacobian=False, chunk=128):
         torch = _torch()
         self.device = torch.device(device or 'cuda')
         self.models = list(models)
@@ -118,11 +118,30 @@ class Batch(object):
             self.run_order = np.argsort(-cost, kind='stable')
         else:
             self.run_order = np.arange(n)
-        items = (_lib.BatchItem * n)()
-        for slot, i in enumerate(self.run_order):
+        # Work items: a model whose trajectories exceed `chunk` (a
+        # thread-mapped block's trajectories per pass) is split into chunks
+        # that different blocks run at once, so a few large models still
+        # fill the GPU and the longest ones do not form the tail alone.
+        spans = []
+        for i in self.run_order:
+            U = int(self.n_traj[i])
+            cs = int(chunk) if chunk else 0
+            if self.mappings[i] == _lib.MAP_WARP:
+                cs = max(cs // 8, 4) if cs else 0
+            if cs and U > cs:
+                k = -(-U // cs)
+                spans += [(i, c * cs, min(cs, U - c * cs), U, k)
+                          for c in range(k)]
+            else:
+                spans.append((i, 0, U, 0, 0))
+        self.n_items = len(spans)
+        self.item_model = np.array([sp[0] for sp in spans], np.int64)
+        self.item_n_traj = np.array([sp[2] for sp in spans], np.int64)
+        items = (_lib.BatchItem * len(spans))()
+        for slot, (i, c0, cn, U, k) in enumerate(spans):
             it = items[slot]
             it.blob_offset = int(self.blob_offset[i])
-            it.n_traj = int(self.n_traj[i])
+            it.n_traj = cn
             it.traj_id_base = int(self.traj_id_base[i])
             it.sample_offset = int(self.sample_offset[i])
             it.traj_offset = int(self.traj_offset[i])
@@ -131,6 +150,10 @@ class Batch(object):
             it.jac_offset = int(self.jac_offset[i])
             it.method = int(self.methods[i])
             it.mapping = int(self.mappings[i])
+            it.chunk_begin = c0
+            it.model_n_traj = U
+            it.group = int(i)
+            it.group_chunks = k
         raw = np.frombuffer(bytes(items), dtype=np.uint8)
         self.d_items = torch.from_numpy(raw.copy()).to(self.device)
         self.d_blobs = torch.from_numpy(
@@ -141,7 +164,7 @@ class Batch(object):
             max(m.n_reactions for m in self.models), 0)
         L = _lib.lib()
         ws = C.c_size_t(0)
-        _lib.check(L.pyst_batch_workspace_size(n, C.byref(ws)),
+        _lib.check(L.pyst_batch_workspace_size(self.n_items, C.byref(ws)),
                    'pyst_batch_workspace_size')
         self.workspace = torch.empty(int(ws.value), dtype=torch.uint8,
                                      device=self.device)
@@ -175,12 +198,12 @@ class Batch(object):
     def run(self, seed=0, stream=None, ssa_fallback_steps=100,
             max_leap_retries=63, step_budget=None, block_size=0):
         """Enqueue the whole batch on ``stream`` (one kernel launch).
-        ``block_size`` 0 picks 64 threads when no item has more than 64
+        ``block_size`` 0 picks 64 threads when no work item has more than 64
         trajectories (one block then covers an item), else 128."""
         torch = _torch()
         L = _lib.lib()
         if not block_size:
-            block_size = 64 if int(self.n_traj.max()) <= 64 else 128
+            block_size = 64 if int(self.item_n_traj.max()) <= 64 else 128
         if step_budget is None:
             step_budget = DEFAULT_STEP_BUDGET
         o = self.out
@@ -200,7 +223,7 @@ class Batch(object):
             stream = torch.cuda.current_stream(self.device)
         _lib.check(L.pyst_batch_run(
             self.d_blobs.data_ptr(), self.d_items.data_ptr(),
-            len(self.models), C.byref(self.limits), C.byref(r),
+            self.n_items, C.byref(self.limits), C.byref(r),
             C.byref(outs), self.workspace.data_ptr(),
             self.workspace.numel(), C.c_void_p(stream.cuda_stream)),
             'pyst_batch_run')

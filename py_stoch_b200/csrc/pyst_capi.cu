@@ -47,6 +47,22 @@ namespace {
 constexpr int kSortedCapSsa = PYST_CAP_SSA;
 constexpr int kSortedCapLeap = PYST_CAP_LEAP;
 
+// The factor and net-change sections of a host blob lie inside it (so the
+// packability check below reads only the blob).
+bool sections_in_blob(const uint32_t* h, int words, int R) {
+  const int64_t fp = h[PYST_H_OFF_FACPTR], f = h[PYST_H_OFF_FAC];
+  const int64_t np = h[PYST_H_OFF_NETPTR], n = h[PYST_H_OFF_NET];
+  if (fp < PYST_H_WORDS_HEADER || fp + R + 1 > words ||
+      np < PYST_H_WORDS_HEADER || np + R + 1 > words)
+    return false;
+  if (f < PYST_H_WORDS_HEADER || n < PYST_H_WORDS_HEADER) return false;
+  for (int j = 0; j <= R; ++j)
+    if (h[fp + j] > h[fp + R] || f + h[fp + j] > words ||
+        h[np + j] > h[np + R] || n + h[np + j] > words)
+      return false;
+  return true;
+}
+
 int read_header(const uint32_t* h, HostModelInfo* mi) {
   if (!h) return PYST_EINVAL;
   if (h[PYST_H_MAGIC] != PYST_BLOB_MAGIC) return PYST_EINVAL;
@@ -59,6 +75,9 @@ int read_header(const uint32_t* h, HostModelInfo* mi) {
   if (mi->S < 1 || mi->R < 1 || mi->S > PYST_MAX_SPECIES ||
       mi->R > PYST_MAX_REACTIONS)
     return PYST_EUNSUPPORTED;
+  mi->packable = mi->nlaw == 0 && sections_in_blob(h, mi->words, mi->R);
+  for (int j = 0; j < mi->R && mi->packable; ++j)
+    mi->packable = blob_reaction_packable(h, j);
   return PYST_OK;
 }
 
@@ -76,6 +95,12 @@ int check_run(const pyst_run_desc* run) {
   if (run->step_budget < 0) return PYST_EINVAL;
   if (run->block_size != 0 &&
       (run->block_size < 32 || run->block_size > 128 || run->block_size % 32))
+    return PYST_EINVAL;
+  if (run->round_ssa < 0 || run->round_leap < 0 || run->pool_slots < 0 ||
+      run->pool_slots > 2 || run->sorted_block < 0 ||
+      (run->sorted_block != 0 &&
+       (run->sorted_block < 64 || run->sorted_block > 896 ||
+        run->sorted_block % 32)))
     return PYST_EINVAL;
   return PYST_OK;
 }
@@ -152,11 +177,16 @@ int single_run(const uint32_t* h_blob, const uint32_t* d_blob,
       !(run->flags & PYST_FLAG_UNSORTED) && mi.nlaw == 0) {
     // (models with general kinetic laws take the simple tau loop: the
     // sorted kernel's engine carries no law evaluator)
+    SortedGeometry g;
+    g.cap_ssa = run->round_ssa ? run->round_ssa : kSortedCapSsa;
+    g.cap_leap = run->round_leap ? run->round_leap : kSortedCapLeap;
+    g.pool = run->pool_slots;
+    g.block = run->sorted_block;
     const int rc =
         score ? launch_tau_sorted_1(mi.R, d_blob, mi, n, idb, ra, ob, queue,
-                                    kSortedCapSsa, kSortedCapLeap, st)
+                                    g, st)
               : launch_tau_sorted_0(mi.R, d_blob, mi, n, idb, ra, ob, queue,
-                                    kSortedCapSsa, kSortedCapLeap, st);
+                                    g, st);
     // the sorted block keeps every slot's species in shared memory; for
     // models with too many species fall back to the unsorted loop
     if (rc != PYST_EUNSUPPORTED) return rc;
@@ -245,7 +275,8 @@ int pyst_tau_leap_run(const uint32_t* h_blob, const uint32_t* d_blob,
 
 int pyst_batch_workspace_size(int64_t n_items, size_t* bytes) {
   if (!bytes || n_items < 0) return PYST_EINVAL;
-  *bytes = PYST_RUN_WORKSPACE_BYTES;  // the work-queue counter, padded
+  // the work-queue counter (padded), then one completion counter per item
+  *bytes = PYST_RUN_WORKSPACE_BYTES + (size_t)n_items * sizeof(uint32_t);
   return PYST_OK;
 }
 
@@ -257,7 +288,9 @@ int pyst_batch_run(const uint32_t* d_blobs, const pyst_batch_item* d_items,
     return PYST_EINVAL;
   if (((uintptr_t)d_blobs & 15) || n_items < 0) return PYST_EINVAL;
   if (!d_workspace || ((uintptr_t)d_workspace & 7)) return PYST_EINVAL;
-  if (workspace_bytes < PYST_RUN_WORKSPACE_BYTES) return PYST_EWORKSPACE;
+  if (workspace_bytes <
+      PYST_RUN_WORKSPACE_BYTES + (size_t)n_items * sizeof(uint32_t))
+    return PYST_EWORKSPACE;
   if (lim->max_blob_words <= 0 || (lim->max_blob_words & 3) ||
       lim->max_blob_words > PYST_MAX_BLOB_WORDS || lim->max_species < 1 ||
       lim->max_reactions < 1 || lim->max_species > PYST_MAX_SPECIES ||
@@ -275,10 +308,16 @@ int pyst_batch_run(const uint32_t* d_blobs, const pyst_batch_item* d_items,
   ob.stride = 0;  // per item
   cudaStream_t st = (cudaStream_t)stream;
   unsigned long long* queue = (unsigned long long*)d_workspace;
+  unsigned* done =
+      (unsigned*)((unsigned char*)d_workspace + PYST_RUN_WORKSPACE_BYTES);
+  if (cudaMemsetAsync(done, 0, (size_t)n_items * sizeof(uint32_t), st) !=
+      cudaSuccess)
+    return PYST_ECUDA;
   if (out->score)
-    return launch_batch_1(d_blobs, d_items, n_items, lim, ra, ob, queue, bs,
-                          st);
-  return launch_batch_0(d_blobs, d_items, n_items, lim, ra, ob, queue, bs, st);
+    return launch_batch_1(d_blobs, d_items, n_items, lim, ra, ob, queue, done,
+                          bs, st);
+  return launch_batch_0(d_blobs, d_items, n_items, lim, ra, ob, queue, done,
+                        bs, st);
 }
 
 int pyst_score_backward_workspace_size(int64_t n_traj, int32_t n_reactions,

@@ -27,14 +27,16 @@ namespace pyst {
 // merged at link time; a per-flavour namespace keeps them apart.
 namespace PYST_CAT(batch_flavour_, PYST_SCORE, ) {
 
-// Summary statistics and score Jacobians of one finished item, computed by
-// the block that ran it from the samples (and scores) it just wrote, sums
-// over trajectories in trajectory order.  Means and variances go to shared
+// Summary statistics and score Jacobians of one finished model (U
+// trajectories), computed by the block that ran it -- or, for a model split
+// into chunks, ran its last chunk -- from the samples (and scores) written
+// for it, sums over trajectories in trajectory order.  Loads bypass L1
+// (other blocks wrote part of the data).  Means and variances go to shared
 // scratch `ms` when 2*kappa*ita doubles fit, else they are recomputed.
 __device__ void item_epilogue(const ModelView& m, const pyst_batch_item& item,
-                              const OutBase& ob, double* ms, int ms_bytes) {
+                              int64_t U, const OutBase& ob, double* ms,
+                              int ms_bytes) {
   const int ita = m.ita, KF = m.kappa * m.ita, R = m.R;
-  const int64_t U = item.n_traj;
   if (U <= 0) return;
   const int32_t* smp = ob.samples + item.sample_offset;
   const double dU = (double)U;
@@ -43,7 +45,7 @@ __device__ void item_epilogue(const ModelView& m, const pyst_batch_item& item,
     const int32_t* row = smp + (int64_t)kf * U;
     double s = 0.0, s2 = 0.0;
     for (int64_t u = 0; u < U; ++u) {
-      const double x = (double)row[u];
+      const double x = (double)__ldcg(row + u);
       s = __dadd_rn(s, x);
       s2 = __dadd_rn(s2, __dmul_rn(x, x));
     }
@@ -67,7 +69,8 @@ __device__ void item_epilogue(const ModelView& m, const pyst_batch_item& item,
         const int32_t* rb = ra_ + U;
         double sab = 0.0;
         for (int64_t u = 0; u < U; ++u)
-          sab = __dadd_rn(sab, __dmul_rn((double)ra_[u], (double)rb[u]));
+          sab = __dadd_rn(sab, __dmul_rn((double)__ldcg(ra_ + u),
+                                         (double)__ldcg(rb + u)));
         const double cov = __dsub_rn(__ddiv_rn(sab, dU), __dmul_rn(mean, mb));
         const double den = __dmul_rn(var, vb);
         if (den > 0.0) corr = __ddiv_rn(cov, __dsqrt_rn(den));
@@ -93,8 +96,8 @@ __device__ void item_epilogue(const ModelView& m, const pyst_batch_item& item,
     const int32_t* row = smp + (int64_t)kf * U;
     double gm = 0.0, gv = 0.0;
     for (int64_t u = 0; u < U; ++u) {
-      const double d = __dsub_rn((double)row[u], mean);
-      const double s = sc[u * R + j];
+      const double d = __dsub_rn((double)__ldcg(row + u), mean);
+      const double s = __ldcg(sc + u * R + j);
       gm = __dadd_rn(gm, __dmul_rn(d, s));
       gv = __dadd_rn(gv, __dmul_rn(__dsub_rn(__dmul_rn(d, d), var), s));
     }
@@ -108,10 +111,11 @@ template <bool SCORE>
 __global__ void PYST_BATCH_BOUNDS
     k_batch(const uint32_t* __restrict__ gblobs,
             const pyst_batch_item* __restrict__ items, int64_t n_items,
-            RunArgs ra, OutBase ob, unsigned long long* queue,
+            RunArgs ra, OutBase ob, unsigned long long* queue, unsigned* done,
             int max_blob_words, int warp_bytes, int dyn_bytes, int pk_bytes) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ long long s_item;
+  __shared__ int s_last;
   uint32_t* sblob = (uint32_t*)smem;
   uint64_t* bar = (uint64_t*)(smem + (size_t)max_blob_words * 4);
   // packed reaction descriptors of the current item (thread mapping)
@@ -131,14 +135,18 @@ __global__ void PYST_BATCH_BOUNDS
     const long long it = s_item;
     if (it >= n_items) break;
     const pyst_batch_item item = items[it];
+    // the model's trajectory count (a split model's chunks share it) and
+    // this item's first trajectory in it
+    const int64_t U = item.model_n_traj > 0 ? item.model_n_traj : item.n_traj;
+    const int64_t cb = item.model_n_traj > 0 ? item.chunk_begin : 0;
     const uint32_t* blob = gblobs + item.blob_offset;
     const int words = (int)__ldg(blob + PYST_H_WORDS);
     const bool ok = stage_blob(sblob, blob, words, bar, parity,
                                ra.stage_polls);
     if (!ok) {
       mbar_drain(bar, parity);
-      for (int64_t u = threadIdx.x; u < item.n_traj; u += bs)
-        mark_staging_failure(ob, item.traj_offset + u);
+      for (int64_t v = threadIdx.x; v < item.n_traj; v += bs)
+        mark_staging_failure(ob, item.traj_offset + cb + v);
       break;
     }
     parity ^= 1u;
@@ -150,9 +158,9 @@ __global__ void PYST_BATCH_BOUNDS
       // scores NaN
       const int KF = m.kappa * m.ita;
       const double nan = __longlong_as_double(0x7ff8000000000000ll);
-      for (int64_t u = threadIdx.x; u < item.n_traj; u += bs) {
-        const TrajOut o = ob.at(item.sample_offset, u, item.traj_offset,
-                                item.score_offset, item.n_traj, m.R);
+      for (int64_t v = threadIdx.x; v < item.n_traj; v += bs) {
+        const TrajOut o = ob.at(item.sample_offset, cb + v, item.traj_offset,
+                                item.score_offset, U, m.R);
         for (int kf = 0; kf < KF; ++kf) o.samples[(int64_t)kf * o.stride] = -1;
         if (o.status) *o.status = (uint8_t)PYST_TRAJ_UNSUPPORTED;
         if (o.events) *o.events = 0;
@@ -172,9 +180,10 @@ __global__ void PYST_BATCH_BOUNDS
         int32_t* xcol = (int32_t*)dyn + threadIdx.x;
         int64_t* slot =
             (int64_t*)((int32_t*)dyn + (size_t)m.S * bs) + threadIdx.x;
-        for (int64_t u = threadIdx.x; u < item.n_traj; u += bs) {
+        for (int64_t v = threadIdx.x; v < item.n_traj; v += bs) {
+          const int64_t u = cb + v;
           const TrajOut o = ob.at(item.sample_offset, u, item.traj_offset,
-                                  item.score_offset, item.n_traj, m.R);
+                                  item.score_offset, U, m.R);
           const uint64_t id = (uint64_t)item.traj_id_base + (uint64_t)u;
           if (m.R <= 8) {
             if (tau) run_thread<8, true, SCORE>(m, xcol, slot, bs, ra, id, o);
@@ -192,9 +201,10 @@ __global__ void PYST_BATCH_BOUNDS
         unsigned char* mine = dyn + (size_t)wid * warp_bytes;
         const WarpSmem ws = warp_smem(mine, m.S, m.R);
         double* sacc = (double*)(mine + warp_smem_bytes(m.S, m.R));
-        for (int64_t u = wid; u < item.n_traj; u += nw) {
+        for (int64_t v = wid; v < item.n_traj; v += nw) {
+          const int64_t u = cb + v;
           const TrajOut o = ob.at(item.sample_offset, u, item.traj_offset,
-                                  item.score_offset, item.n_traj, m.R);
+                                  item.score_offset, U, m.R);
           const uint64_t id = (uint64_t)item.traj_id_base + (uint64_t)u;
           if (tau) run_warp<true, SCORE>(m, ws, ra, id, o, sacc);
           else run_warp<false, SCORE>(m, ws, ra, id, o, sacc);
@@ -202,8 +212,22 @@ __global__ void PYST_BATCH_BOUNDS
       }
     }
     if (ob.stats || ob.jac) {
+      // a split model: every thread makes its outputs visible device-wide
+      // before the chunk is counted (uniform branch)
+      if (item.group_chunks > 1) __threadfence();
       __syncthreads();  // the item's samples are all written
-      item_epilogue(m, item, ob, (double*)dyn, dyn_bytes);
+      bool last = true;
+      if (item.group_chunks > 1) {
+        // the block finishing the model's last chunk reduces the model
+        if (threadIdx.x == 0) {
+          s_last = atomicAdd(done + item.group, 1u) + 1u ==
+                   (unsigned)item.group_chunks;
+          if (s_last) __threadfence();
+        }
+        __syncthreads();
+        last = s_last != 0;
+      }
+      if (last) item_epilogue(m, item, U, ob, (double*)dyn, dyn_bytes);
     }
     __syncthreads();  // everyone done with sblob and dyn before restaging
   }
@@ -215,7 +239,7 @@ using namespace PYST_CAT(batch_flavour_, PYST_SCORE, );
 int PYST_CAT(launch_batch_, PYST_SCORE, )(
     const uint32_t* d_blobs, const pyst_batch_item* d_items, int64_t n_items,
     const pyst_batch_limits* lim, const RunArgs& ra, const OutBase& ob,
-    unsigned long long* queue, int bs, cudaStream_t st) {
+    unsigned long long* queue, unsigned* done, int bs, cudaStream_t st) {
   const size_t wb =
       host_warp_bytes(lim->max_species, lim->max_reactions, PYST_SCORE);
   const size_t thread_bytes = (size_t)bs * lim->max_species * 12;
@@ -239,8 +263,8 @@ int PYST_CAT(launch_batch_, PYST_SCORE, )(
   int64_t grid = (int64_t)num_sms() * per_sm;
   if (grid > n_items) grid = n_items;
   kf<<<(unsigned)grid, bs, smem, st>>>(d_blobs, d_items, n_items, ra, ob,
-                                       queue, lim->max_blob_words, (int)wb,
-                                       (int)dyn, (int)pk_bytes);
+                                       queue, done, lim->max_blob_words,
+                                       (int)wb, (int)dyn, (int)pk_bytes);
   return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
 }
 

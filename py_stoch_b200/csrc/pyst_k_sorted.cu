@@ -356,17 +356,25 @@ __global__ void __launch_bounds__(kMaxBlock, kMinBlocks)
 template <int MR>
 int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
                uint64_t id_base, const RunArgs& ra, const OutBase& ob,
-               unsigned long long* queue, cudaStream_t st, int cap_ssa,
-               int cap_leap) {
+               unsigned long long* queue, cudaStream_t st,
+               const SortedGeometry& g) {
   const int maxr = MR > 0 ? MR : 1;
-  // the largest block up to the preferred size whose pools fit, first with
-  // kMaxPool slots per thread, then with one
+  // the largest block (whole warps) up to the preferred size whose pools
+  // fit, first with the preferred slots per thread, then with one
+  const int pref_block = g.block ? (g.block < kMaxBlock ? g.block : kMaxBlock)
+                                 : kPrefBlock;
+  const int pref_pool = g.pool ? (g.pool < kMaxPool ? g.pool : kMaxPool)
+                               : kMaxPool;
+  static const int kBlocks[] = {896, 768, 640, 512, 448, 384, 320, 256,
+                                224, 192, 160, 128, 96, 64};
   int pool = 0, block = 0;
-  for (int p = kMaxPool; p >= 1 && !block; --p)
-    for (int b = kPrefBlock; b >= 64 && !block; b >>= 1)
-      if (sorted_smem_bytes(mi.words, mi.S, maxr, p, b) <= kMaxDynSmem) {
+  for (int p = pref_pool; p >= 1 && !block; --p)
+    for (int b : kBlocks)
+      if (b <= pref_block &&
+          sorted_smem_bytes(mi.words, mi.S, maxr, p, b) <= kMaxDynSmem) {
         pool = p;
         block = b;
+        break;
       }
   if (!block) return PYST_EUNSUPPORTED;
   const size_t smem = sorted_smem_bytes(mi.words, mi.S, maxr, pool, block);
@@ -386,7 +394,8 @@ int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
   const int64_t cap = (int64_t)num_sms() * per_sm;
   if (grid > cap) grid = cap;
   kf<<<(unsigned)grid, block, smem, st>>>(d_blob, mi.words, n, id_base, ra,
-                                          ob, queue, cap_ssa, cap_leap, pool);
+                                          ob, queue, g.cap_ssa, g.cap_leap,
+                                          pool);
   return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
 }
 
@@ -396,26 +405,19 @@ using namespace PYST_CAT(sorted_flavour_, PYST_SCORE, );
 int PYST_CAT(launch_tau_sorted_, PYST_SCORE, )(
     int maxr, const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
     uint64_t id_base, const RunArgs& ra, const OutBase& ob,
-    unsigned long long* queue, int cap_ssa, int cap_leap, cudaStream_t st) {
+    unsigned long long* queue, const SortedGeometry& g, cudaStream_t st) {
   if (n <= 0) return PYST_OK;
 #if !PYST_SCORE
   if (maxr > PYST_THREAD_MAX_REACTIONS)
-    return launch_one<0>(d_blob, mi, n, id_base, ra, ob, queue, st, cap_ssa,
-                         cap_leap);
+    return launch_one<0>(d_blob, mi, n, id_base, ra, ob, queue, st, g);
 #else
   if (maxr > PYST_THREAD_MAX_REACTIONS) return PYST_EUNSUPPORTED;
 #endif
-  if (maxr <= 4)
-    return launch_one<4>(d_blob, mi, n, id_base, ra, ob, queue, st, cap_ssa,
-                         cap_leap);
-  if (maxr <= 8)
-    return launch_one<8>(d_blob, mi, n, id_base, ra, ob, queue, st, cap_ssa,
-                         cap_leap);
+  if (maxr <= 4) return launch_one<4>(d_blob, mi, n, id_base, ra, ob, queue, st, g);
+  if (maxr <= 8) return launch_one<8>(d_blob, mi, n, id_base, ra, ob, queue, st, g);
   if (maxr <= 16)
-    return launch_one<16>(d_blob, mi, n, id_base, ra, ob, queue, st, cap_ssa,
-                          cap_leap);
-  return launch_one<32>(d_blob, mi, n, id_base, ra, ob, queue, st, cap_ssa,
-                        cap_leap);
+    return launch_one<16>(d_blob, mi, n, id_base, ra, ob, queue, st, g);
+  return launch_one<32>(d_blob, mi, n, id_base, ra, ob, queue, st, g);
 }
 
 }  // namespace pyst

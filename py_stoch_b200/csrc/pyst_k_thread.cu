@@ -110,8 +110,8 @@ constexpr int kGroupMaxPerSm = 16;
 // j_1 .. j_d, computes its propensities, total, tau and selection for step
 // d + 1 (with step d + 1's random numbers), and a few ballots publish every
 // lane's selection, so each lane walks the tree from the root along the
-// selections to the true path.  Lanes per depth grow as R^d; D is the
-// largest depth with 1 + R + ... + R^(D-1) <= 32 (at most kSpecMaxDepth):
+// selections to the true path.  Lanes per depth grow as R^d, so the depth
+// D is 5 for R <= 2 (31 lanes), 3 for R <= 4 (21) and 2 for R <= 8 (9):
 // Lotka-Volterra (R = 3) advances 3 steps per pass on 13 lanes.
 // The passes commit only when none of the D steps reaches a sample time,
 // absorbs, runs out of step budget or leaves the int32 range; otherwise D
@@ -120,8 +120,6 @@ constexpr int kGroupMaxPerSm = 16;
 // step it evaluates, so results are those of one thread per trajectory,
 // bit for bit.  Species counts (at most MAXS) live in registers, read and
 // written by unrolled selects.
-constexpr int kSpecMaxDepth = 5;
-
 template <int MAXS>
 __device__ __forceinline__ int reg_get(const int (&x)[MAXS], int sp) {
   int v = x[0];
@@ -197,22 +195,25 @@ __device__ __forceinline__ void step_variates(Stream& rs, uint64_t blk,
   u = u53(w.z, w.w);
 }
 
+// Lanes of a D-level tree for R reactions: 1 + R + ... + R^(D-1).
+__host__ __device__ constexpr int spec_lanes(int R, int D) {
+  return D <= 0 ? 0 : 1 + R * spec_lanes(R, D - 1);
+}
+
 // One whole trajectory by the calling warp (all 32 lanes; lane 0 writes).
-template <int MAXR, int MAXS>
+// D levels (compile time; the caller checks spec_lanes(R, D) <= 32), at
+// most MAXS species in registers.
+template <int MAXR, int MAXS, int D>
 __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
                               uint64_t traj_id, const TrajOut& o) {
   const int R = m.R, S = m.S, ita = m.ita, kappa = m.kappa;
   const int lane = threadIdx.x & 31;
-  // tree shape: D levels, lanes [start_d, start_d + R^d) at depth d
-  int D = 1, used = 1, width = 1;
-  while (D < kSpecMaxDepth && used + width * R <= 32) {
-    width *= R;
-    used += width;
-    ++D;
-  }
+  // this lane's depth dl and path j_1 .. j_dl (base-R digits of its index
+  // within the depth, first firing first)
   int dl = 0, il = 0;
   {
     int st = 0, w = 1;
+#pragma unroll
     for (int d = 0; d < D; ++d) {
       if (lane >= st && lane < st + w) {
         dl = d;
@@ -222,21 +223,36 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
       w *= R;
     }
   }
-  // this lane's path j_1 .. j_dl: base-R digits of il, first firing first
-  int path[kSpecMaxDepth];
-  {
-    int v = il;
+  const bool in_tree = lane < spec_lanes(R, D);
+  // the path's net change, and the extremes of its running sum, per species
+  // (the states along the path stay in [0, 2^31) iff x + lo >= 0 and
+  // x + hi < 2^31), fixed for the whole trajectory
+  int dx[MAXS], lo[MAXS], hi[MAXS];
 #pragma unroll
-    for (int k = kSpecMaxDepth - 1; k >= 0; --k) {
-      if (k < dl) {
-        path[k] = v % R;
-        v /= R;
-      } else {
-        path[k] = 0;
+  for (int s = 0; s < MAXS; ++s) dx[s] = lo[s] = hi[s] = 0;
+  {
+    int pw = 1;
+    for (int k = 1; k < dl; ++k) pw *= R;
+    for (int k = 0; k < dl; ++k) {
+      const int j = (il / pw) % R;
+      pw = pw > 1 ? pw / R : 1;
+      const uint32_t d = m.pk[R + j];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        if (q < pnet_count(d)) {
+          const int sp = pnet_species(d, q);
+#pragma unroll
+          for (int s = 0; s < MAXS; ++s) {
+            if (s == sp) {
+              dx[s] += pnet_delta(d, q);
+              lo[s] = dx[s] < lo[s] ? dx[s] : lo[s];
+              hi[s] = dx[s] > hi[s] ? dx[s] : hi[s];
+            }
+          }
+        }
       }
     }
   }
-  const bool in_tree = lane < used;
 
   Stream rs = make_stream(ra.seed, traj_id);
   int x[MAXS];
@@ -276,15 +292,15 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
       step_variates(rs, vb + 32u + (uint64_t)lane, e_n, u_n);
     }
     bool committed = false;
-    if (D > 1) {
+    if (D > 1 && steps + D <= budget) {
       // ---- every lane: the step at the end of its path --------------
       int xs[MAXS];
-#pragma unroll
-      for (int s = 0; s < MAXS; ++s) xs[s] = x[s];
       bool ok = in_tree;
 #pragma unroll
-      for (int k = 0; k < kSpecMaxDepth; ++k)
-        if (k < dl) ok &= reg_apply(xs, m.pk[R + path[k]]);
+      for (int s = 0; s < MAXS; ++s) {
+        xs[s] = x[s] + dx[s];
+        ok &= x[s] + lo[s] >= 0 && x[s] <= (int)PYST_I32MAX - hi[s];
+      }
       float a[MAXR];
       const double a0 = reg_propensities<MAXR>(m, xs, a);
       double e, u;
@@ -292,61 +308,49 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
       const double tau = __ddiv_rn(e, a0);
       const int sel = select_reaction<MAXR>(a, R, __dmul_rn(u, a0));
       ok &= a0 != 0.0;
+      // the state after this lane's step (needed from the deepest lane of
+      // the true path): its range check joins the lane's flag
+      if (dl == D - 1) ok &= reg_apply(xs, m.pk[R + (sel < 0 ? 0 : sel)]);
       unsigned sb[kSelBits];
 #pragma unroll
       for (int b = 0; b < kSelBits; ++b)
         sb[b] = __ballot_sync(0xffffffffu, (sel >> b) & 1);
       const unsigned bad = __ballot_sync(0xffffffffu, !ok);
       // ---- walk the tree along the selections (uniform) ---------------
-      int J[kSpecMaxDepth], L[kSpecMaxDepth];
-      bool walk = true;
+      int J[D], L[D];
+      unsigned badpath = 0u;
       {
         int i = 0, st = 0, w = 1;
 #pragma unroll
-        for (int d = 0; d < kSpecMaxDepth; ++d) {
-          if (d < D && walk) {
-            const int ln = st + i;
-            if ((bad >> ln) & 1u) walk = false;
-            int j = 0;
+        for (int d = 0; d < D; ++d) {
+          const int ln = st + i;
+          badpath |= (bad >> ln) & 1u;
+          int j = 0;
 #pragma unroll
-            for (int b = 0; b < kSelBits; ++b) j |= (int)((sb[b] >> ln) & 1u) << b;
-            J[d] = j;
-            L[d] = ln;
-            i = i * R + j;
-            st += w;
-            w *= R;
-          } else {
-            J[d] = 0;
-            L[d] = 0;
-          }
+          for (int b = 0; b < kSelBits; ++b)
+            j |= (int)((sb[b] >> ln) & 1u) << b;
+          J[d] = j;
+          L[d] = ln;
+          i = i * R + j;
+          st += w;
+          w *= R;
         }
       }
-      if (walk && steps + D <= budget) {
+      if (!badpath) {
         double tt = t;
 #pragma unroll
-        for (int d = 0; d < kSpecMaxDepth; ++d) {
-          const double td = __shfl_sync(0xffffffffu, tau, L[d]);
-          if (d < D) tt = __dadd_rn(tt, td);
-        }
+        for (int d = 0; d < D; ++d)
+          tt = __dadd_rn(tt, __shfl_sync(0xffffffffu, tau, L[d]));
         if (tt < tf) {
-          int xn[MAXS];
 #pragma unroll
-          for (int s = 0; s < MAXS; ++s) xn[s] = x[s];
-          bool inr = true;
+          for (int s = 0; s < MAXS; ++s)
+            x[s] = __shfl_sync(0xffffffffu, xs[s], L[D - 1]);
 #pragma unroll
-          for (int d = 0; d < kSpecMaxDepth; ++d)
-            if (d < D) inr &= reg_apply(xn, m.pk[R + J[d]]);
-          if (inr) {
-#pragma unroll
-            for (int s = 0; s < MAXS; ++s) x[s] = xn[s];
-#pragma unroll
-            for (int d = 0; d < kSpecMaxDepth; ++d)
-              if (d < D) h = seq_mix(h, (uint64_t)J[d]);
-            t = tt;
-            steps += D;
-            events += D;
-            committed = true;
-          }
+          for (int d = 0; d < D; ++d) h = seq_mix(h, (uint64_t)J[d]);
+          t = tt;
+          steps += D;
+          events += D;
+          committed = true;
         }
       }
     }
@@ -409,6 +413,76 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
 // species held in registers by the lane tree
 constexpr int kSpecMaxSpecies = 8;
 
+// One warp per trajectory, the lane tree (D levels, at most MAXS species);
+// launched only for models whose every reaction packs
+// (blob_reaction_packable) with at most MAXS species.  4 blocks of 128
+// threads per SM: a run of 148 x 16 trajectories is resident at once.
+template <int MAXR, int MAXS, int D>
+__global__ void __launch_bounds__(128, 4)
+    k_plain_tree(const uint32_t* __restrict__ gblob, int blob_words,
+                 int64_t n_traj, uint64_t id_base, RunArgs ra, OutBase ob) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint32_t* sblob = (uint32_t*)smem;
+  uint64_t* bar = (uint64_t*)(smem + (size_t)blob_words * 4);
+  uint32_t* pk = (uint32_t*)(smem + (size_t)blob_words * 4 + 16);
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const bool ok = stage_blob(sblob, gblob, blob_words, bar, 0,
+                             ra.stage_polls);
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const bool leader = (threadIdx.x & 31) == 0;
+  int64_t u = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  if (!ok) {
+    mbar_drain(bar, 0);  // let a late copy land before the block exits
+    for (; u < n_traj; u += nwarps)
+      if (leader) mark_staging_failure(ob, u);
+    return;
+  }
+  ModelView m;
+  m.load(sblob);
+  m.pk = pk;
+  // the host launches this kernel only when every reaction packs, and the
+  // device packer decides with the same predicate
+  m.fast = __syncthreads_and(pack_reactions(m, pk)) != 0;
+  for (; u < n_traj; u += nwarps) {
+    const TrajOut o = ob.at(0, u, 0, 0, ob.stride, m.R);
+    run_spec_tree<MAXR, MAXS, D>(m, ra, id_base + (uint64_t)u, o);
+  }
+}
+
+template <int MAXR, int MAXS, int D>
+int launch_tree(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
+                uint64_t id_base, const RunArgs& ra, const OutBase& ob,
+                cudaStream_t st) {
+  auto kf = k_plain_tree<MAXR, MAXS, D>;
+  const size_t smem = (size_t)mi.words * 4 + 16 + packed_bytes(mi.R);
+  const int rc = set_smem(kf, smem);
+  if (rc) return rc;
+  const int bs = 128;
+  const int64_t grid = (n * 32 + bs - 1) / bs;
+  kf<<<(unsigned)grid, bs, smem, st>>>(d_blob, mi.words, n, id_base, ra, ob);
+  return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
+}
+
+// The lane tree for a packable model of at most 8 reactions and
+// kSpecMaxSpecies species: depth 5 for R <= 2, 3 for R <= 4, 2 for R <= 8.
+int launch_tree_for(const uint32_t* d_blob, const HostModelInfo& mi,
+                    int64_t n, uint64_t id_base, const RunArgs& ra,
+                    const OutBase& ob, cudaStream_t st) {
+  const bool s4 = mi.S <= 4;
+  if (mi.R <= 2)
+    return s4 ? launch_tree<4, 4, 5>(d_blob, mi, n, id_base, ra, ob, st)
+              : launch_tree<4, 8, 5>(d_blob, mi, n, id_base, ra, ob, st);
+  if (mi.R <= 4)
+    return s4 ? launch_tree<4, 4, 3>(d_blob, mi, n, id_base, ra, ob, st)
+              : launch_tree<4, 8, 3>(d_blob, mi, n, id_base, ra, ob, st);
+  return s4 ? launch_tree<8, 4, 2>(d_blob, mi, n, id_base, ra, ob, st)
+            : launch_tree<8, 8, 2>(d_blob, mi, n, id_base, ra, ob, st);
+}
+
 template <int MAXR, int LG>
 __global__ void __launch_bounds__(128)
     k_plain_group(const uint32_t* __restrict__ gblob, int blob_words,
@@ -442,16 +516,9 @@ __global__ void __launch_bounds__(128)
   m.fast = __syncthreads_and(pack_reactions(m, pk)) != 0;
   int32_t* xcol = xbase + threadIdx.x;
   int64_t* slot = (int64_t*)(xbase + (size_t)m.S * bs) + threadIdx.x;
-  // the lane tree needs a whole warp, packed reactions and few species
-  const bool tree = LG == 32 && m.fast && m.S <= kSpecMaxSpecies &&
-                    PYST_SPEC_TREE;
   for (; u < n_traj; u += ngroups) {
     const TrajOut o = ob.at(0, u, 0, 0, ob.stride, m.R);
     const uint64_t id = id_base + (uint64_t)u;
-    if (tree) {
-      run_spec_tree<MAXR, kSpecMaxSpecies>(m, ra, id, o);
-      continue;
-    }
     TState st;
     thread_init<false>(m, xcol, bs, st);
     double integ[1] = {0.0};
@@ -525,6 +592,8 @@ int PYST_CAT(launch_plain_thread_, PYST_TAU, PYST_SCORE)(
   // fewer trajectories than one 128-thread block of lane groups per SM
   if (maxr <= 8 && bs <= 128 && bs % kGroupLanes == 0 &&
       n <= (int64_t)num_sms() * kGroupMaxPerSm) {
+    if (PYST_SPEC_TREE && mi.packable && mi.S <= kSpecMaxSpecies)
+      return launch_tree_for(d_blob, mi, n, id_base, ra, ob, st);
     if (maxr <= 4)
       return launch_group<4>(d_blob, mi, n, id_base, ra, ob, bs, st, smem);
     return launch_group<8>(d_blob, mi, n, id_base, ra, ob, bs, st, smem);

@@ -48,7 +48,8 @@ __device__ __forceinline__ void mark_staging_failure(const OutBase& ob,
 
 struct HostModelInfo {
   int S, R, words;
-  int nlaw;  // reactions with a general kinetic law
+  int nlaw;       // reactions with a general kinetic law
+  bool packable;  // every reaction fits the packed descriptors (no laws)
 };
 
 constexpr size_t kMaxDynSmem = 227 * 1024;
@@ -109,18 +110,24 @@ PYST_DECL_WARP(1, 1)
   int launch_batch_##SC(const uint32_t* d_blobs,                             \
                         const pyst_batch_item* d_items, int64_t n_items,     \
                         const pyst_batch_limits* lim, const RunArgs& ra,     \
-                        const OutBase& ob, unsigned long long* queue, int bs,\
-                        cudaStream_t st);
+                        const OutBase& ob, unsigned long long* queue,       \
+                        unsigned* done, int bs, cudaStream_t st);
 PYST_DECL_BATCH(0)
 PYST_DECL_BATCH(1)
 #undef PYST_DECL_BATCH
+
+// Geometry of the mode-sorted kernel: round lengths, and the preferred
+// slots per thread and block size (0: the kernel's defaults).
+struct SortedGeometry {
+  int cap_ssa, cap_leap, pool, block;
+};
 
 #define PYST_DECL_SORTED(SC)                                                 \
   int launch_tau_sorted_##SC(int maxr, const uint32_t* d_blob,               \
                              const HostModelInfo& mi, int64_t n,             \
                              uint64_t id_base, const RunArgs& ra,            \
                              const OutBase& ob, unsigned long long* queue,   \
-                             int cap_ssa, int cap_leap, cudaStream_t st);
+                             const SortedGeometry& g, cudaStream_t st);
 PYST_DECL_SORTED(0)
 PYST_DECL_SORTED(1)
 #undef PYST_DECL_SORTED

@@ -79,14 +79,18 @@ def simulate(model, n_traj, method='direct', seed=0, traj_id_base=0,
              mapping='auto', device=None, stream=None, status=True,
              events=True, seqhash=False, t_final=False, score=False,
              step_budget=DEFAULT_STEP_BUDGET, ssa_fallback_steps=100, max_leap_retries=63,
-             block_size=0, out=None, d_blob=None, sorted_blocks=True):
+             block_size=0, out=None, d_blob=None, sorted_blocks=True,
+             geometry=None):
     """Run ``n_traj`` trajectories of ``model`` (a :class:`Model`) on the GPU.
 
     Asynchronous on ``stream`` (default: torch's current stream).  ``out``
     may supply preallocated tensors by name; ``d_blob`` a device copy of
     ``model.blob()``.  ``sorted_blocks=False`` selects the simple
     one-trajectory-per-thread tau-leaping loop instead of the mode-sorted
-    block scheduler (identical results).
+    block scheduler (identical results).  ``geometry`` may set the sorted
+    scheduler's ``round_ssa``, ``round_leap``, ``pool_slots`` and
+    ``sorted_block`` (see :class:`py_stoch_b200.autotune.Autotuner`); it
+    changes the speed, never the results.
     """
     torch = _torch()
     if score and getattr(model, 'has_laws', False):
@@ -124,10 +128,17 @@ def simulate(model, n_traj, method='direct', seed=0, traj_id_base=0,
                      sh.data_ptr() if sh is not None else 0,
                      tf.data_ptr() if tf is not None else 0,
                      sc.data_ptr() if sc is not None else 0)
+    geo = dict(geometry or {})
     r = _lib.RunDesc(n, int(traj_id_base), int(seed) & 0xFFFFFFFFFFFFFFFF,
                      meth, _mapping(mapping), int(ssa_fallback_steps),
                      int(max_leap_retries), int(step_budget), int(block_size),
-                     0 if sorted_blocks else _lib.FLAG_UNSORTED)
+                     0 if sorted_blocks else _lib.FLAG_UNSORTED,
+                     int(geo.pop('round_ssa', 0)),
+                     int(geo.pop('round_leap', 0)),
+                     int(geo.pop('pool_slots', 0)),
+                     int(geo.pop('sorted_block', 0)))
+    if geo:
+        raise ValueError('unknown geometry keys: %s' % sorted(geo))
     if stream is None:
         stream = torch.cuda.current_stream(device)
     sptr = C.c_void_p(stream.cuda_stream)

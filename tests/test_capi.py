@@ -35,7 +35,7 @@ def test_exports_every_declared_symbol(built_lib):
 
 
 def test_version_and_strings(built_lib):
-    assert built_lib.pyst_abi_version() == 2
+    assert built_lib.pyst_abi_version() == _lib.ABI_VERSION == 3
     for code in range(6):
         assert built_lib.pyst_status_string(code) != b'unknown status'
     for code in range(9):
@@ -44,7 +44,7 @@ def test_version_and_strings(built_lib):
 
 
 def _run_args():
-    r = _lib.RunDesc(16, 0, 1, 0, 0, 100, 63, 0, 0, 0)
+    r = _lib.RunDesc(16, 0, 1, 0, 0, 100, 63, 0, 0, 0, 0, 0, 0, 0)
     o = _lib.Outputs(0, 0, 0, 0, 0, 0, 0)
     return r, o
 
@@ -88,6 +88,17 @@ def test_run_rejects_bad_arguments(built_lib):
     r.block_size = 100
     assert L.pyst_tau_leap_run(blob.ctypes.data, 16, C.byref(r), C.byref(o),
                                8, 256, None) == _lib.PYST_EINVAL
+    r.block_size = 0
+    # sorted-scheduler geometry: slots 1..2, blocks 64..896 in whole warps
+    for field, bad in (('pool_slots', 3), ('pool_slots', -1),
+                       ('sorted_block', 32), ('sorted_block', 100),
+                       ('sorted_block', 928), ('round_ssa', -1),
+                       ('round_leap', -2)):
+        setattr(r, field, bad)
+        assert L.pyst_tau_leap_run(blob.ctypes.data, 16, C.byref(r),
+                                   C.byref(o), 8, 256,
+                                   None) == _lib.PYST_EINVAL, field
+        setattr(r, field, 0)
     # thread mapping with scores on a model with too many reactions
     big = networks.synthetic_networks(1, seed=1, r_range=(100, 100))[0]
     r.block_size = 0
@@ -145,10 +156,18 @@ def test_batch_and_backward_reject(built_lib):
                             C.byref(o), None, 0, None) == _lib.PYST_EINVAL
     o.samples = 4096
     assert L.pyst_batch_run(16, 16, 1, C.byref(lim), C.byref(r), C.byref(o),
-                            8, 256, None) == _lib.PYST_EUNSUPPORTED
+                            8, 512, None) == _lib.PYST_EUNSUPPORTED
     lim = _lib.BatchLimits(64, 1, 1, 0)
     assert L.pyst_batch_run(16, 16, 1, C.byref(lim), C.byref(r), C.byref(o),
                             8, 8, None) == _lib.PYST_EWORKSPACE
+    # the workspace holds a completion counter per item (split models)
+    ws = C.c_size_t(0)
+    assert L.pyst_batch_workspace_size(1000, C.byref(ws)) == 0
+    assert ws.value == _lib.RUN_WORKSPACE_BYTES + 4 * 1000
+    assert L.pyst_batch_run(16, 16, 1000, C.byref(lim), C.byref(r),
+                            C.byref(o), 8, ws.value - 1,
+                            None) == _lib.PYST_EWORKSPACE
+    assert C.sizeof(_lib.BatchItem) == 96
     ws = C.c_size_t(0)
     assert L.pyst_score_backward_workspace_size(1000, 6, C.byref(ws)) == 0
     assert ws.value == 4 * 6 * 8

@@ -328,6 +328,40 @@ def test_sorted_scheduler_matches_unsorted(torch_cuda, built_lib, oracle_mod,
              score=score)
 
 
+@pytest.mark.parametrize('mapping', ['thread', 'warp'])
+def test_split_models_match_unsplit(torch_cuda, built_lib, oracle_mod,
+                                    mapping):
+    """Models split into chunks that different blocks run (and whose
+    statistics the last chunk's block reduces) give the unsplit batch's
+    outputs bit for bit, and the oracle's."""
+    from py_stoch_b200.batch import Batch
+    models = [networks.schlogl(t_end=1.0, n_samples=9),
+              networks.telegraph(t_end=3.0, n_samples=6),
+              networks.lotka_volterra(t_end=0.2, n_samples=5)]
+    n_traj = [300, 257, 70]
+    outs = []
+    for chunk in (0, 128, 7):
+        b = Batch(models, n_traj, method=['tau', 'direct', 'tau'],
+                  mapping=mapping, score=True, stats=True, jacobian=True,
+                  seqhash=True, chunk=chunk)
+        if chunk == 7:
+            assert b.n_items > 60
+        b.run(seed=13)
+        torch_cuda.cuda.synchronize()
+        outs.append({k: v.cpu().numpy() for k, v in b.out.items()})
+        if chunk == 128:
+            for i, m in enumerate(models):
+                o = oracle_mod.simulate(
+                    m, n_traj[i], 1 if i != 1 else 0, seed=13,
+                    traj_id_base=int(b.traj_id_base[i]),
+                    warp=mapping == 'warp')
+                np.testing.assert_array_equal(b.samples(i).cpu().numpy(),
+                                              o['samples'])
+    for other in outs[1:]:
+        for k, v in outs[0].items():
+            np.testing.assert_array_equal(other[k], v, err_msg=k)
+
+
 def test_batch_stats_and_jacobian(torch_cuda, built_lib):
     """In-kernel per-item statistics and score Jacobians equal the same
     reductions done in NumPy on the batch's own samples and scores."""
