@@ -326,16 +326,23 @@ def batch_vs_plain(kind, dev, subset=256, steps=1, full=True, budget=20000):
                   device=dev, score=grad, stats=grad, jacobian=grad,
                   traj_id_base=ids)
         g = b.graph(seed=11, step_budget=budget)
+        g.replay()  # untimed: the first replay after capture ran slower
+        clk = ClockSampler(dev.index or 0)
+        clk.start()
         tot_ms, ev, ev_ok = 0.0, 0.0, 0.0
         for _ in range(steps):
             ms_, _ = _events_timed(g.replay, stream)
             tot_ms += ms_
             ev += float(b.out['events'].sum().item())
             ev_ok += completed_events(b.out['events'], b.out['status'])
+        clocks = clk.stop()
         st = torch.bincount(b.out['status'].long(), minlength=9).tolist()
         del g
-        return _form_record(tot_ms / steps, ev / steps, ev_ok / steps, st,
-                            len(ms), n_traj, 1)
+        rec = _form_record(tot_ms / steps, ev / steps, ev_ok / steps, st,
+                           len(ms), n_traj, 1)
+        rec['work_items'] = int(b.n_items)
+        rec['clocks'] = clocks
+        return rec
 
     ids = [i * n_traj for i in pick]
     res['batched_same_models'] = batched(sub, ids)
@@ -514,7 +521,8 @@ def ops_roofline(events_per_s, model, mix, peaks, tau, grad=False):
 # ---------------------------------------------------------------------------
 # plain single-model workloads
 # ---------------------------------------------------------------------------
-def run_plain(wl, steps, warmup, dev, world=1, rank=0, e2e=True):
+def run_plain(wl, steps, warmup, dev, world=1, rank=0, e2e=True,
+              geometry=None):
     """Time `steps` simulations of workload `wl` (one kernel launch each,
     plus the score reduction for gradient workloads) after `warmup`
     untimed ones; L2 flushed before every step; device time by CUDA events
@@ -543,7 +551,7 @@ def run_plain(wl, steps, warmup, dev, world=1, rank=0, e2e=True):
     def step(seed, d_blob=None):
         res = simulate(m, n, method=meth, seed=seed, traj_id_base=base,
                        device=dev, stream=stream, out=out, score=grad,
-                       d_blob=d_blob)
+                       d_blob=d_blob, geometry=geometry)
         if grad:
             # backward of mean + var of every sample: the score reduction
             mean, var = _moments(res['samples'])
@@ -683,10 +691,19 @@ def cpu_baseline(wl, check=None, target_s=12.0, threads=0):
 def plain_record(name, wl, args, dev, peaks, steps, warmup, world=1,
                  rank=0):
     """One workload's numbers: device-timed value, e2e, the instruction
-    roofline and, on one GPU, the CPU baseline with the output check."""
-    r = run_plain(wl, steps, warmup, dev, world, rank)
+    roofline and, on one GPU, the CPU baseline with the output check.
+    Tau-leaping workloads run with the mode-sorted scheduler geometry the
+    autotuner picks for them (measured before the timed region)."""
+    geometry = None
+    if wl['method'] == 'tau':
+        from py_stoch_b200.autotune import Autotuner
+        geometry = Autotuner(device=dev).tune_geometry(wl['model'], wl['n'],
+                                                       'tau')
+    r = run_plain(wl, steps, warmup, dev, world, rank, geometry=geometry)
     last = r.pop('_last', None)
     rec = {'workload': wl['desc'], 'trajectories_per_gpu': wl['n']}
+    if geometry:
+        rec['geometry'] = geometry
     rec.update(r)
     if world == 1 and not args.no_cpu_baseline:
         cb, mix = cpu_baseline(wl, check=last)
@@ -780,6 +797,7 @@ def main():
             'data': 'synthetic',
             'config': {'workload': wl['desc'],
                        'trajectories_per_gpu': wl['n'],
+                       'sorted_geometry': head.get('geometry'),
                        'l2': 'flushed (256 MiB write) before every step',
                        'parallelism': 'trajectory shards, one per GPU'},
             'trajectories_per_s': head['trajectories_per_s'],
@@ -827,7 +845,7 @@ def other_configs(args, dev, peaks):
 # steps; the synthetic networks include explosive ones that no budget
 # finishes (10x the budget: 6x the time, 3% more completed firings), so
 # they keep 20,000 steps and report the unfinished fraction.
-FORMS = {'sweep': (64, 2_000_000), 'synthetic': (32, 20_000)}
+FORMS = {'sweep': (64, 2_000_000), 'synthetic': (256, 20_000)}
 
 
 def forms_main(args):

@@ -340,7 +340,9 @@ int pyst_score_combine(const double* d_part, int64_t n_blocks,
  * that -- ceil(n_traj / 256) * n_reactions * 8 bytes, i.e. n_traj up to
  * 1,048,576 with 32 reactions -- return PYST_EUNSUPPORTED.  The first call
  * on a device looks up the array's device address there (make that first
- * call before any stream capture).  All calls share the one array, which
+ * call before any stream capture) and keeps it for the life of the
+ * process, which assumes the device's primary context lives as long: after
+ * a cudaDeviceReset, reload the library.  All calls share the one array, which
  * keeps the last call's contents; calls that overlap on the GPU race, so
  * serialise them (one stream, or events).  This entry point has no
  * counterpart in the reference, which has no gradients. */

@@ -42,6 +42,11 @@ int pyst_test_poisson(const float* d_lam, int64_t n, uint64_t seed,
 int pyst_test_pipe(int32_t which, int32_t iters, int32_t blocks,
                    double* d_sink, void* stream);
 
+/* 1 if every reaction of the host blob fits the packed per-reaction
+ * descriptors (the host's choice of the lane-tree kernel), 0 if not,
+ * minus a PYST_E* code for a bad blob. */
+int pyst_test_model_packable(const uint32_t* h_blob);
+
 /* Bound of the model-staging wait of every later run call in this process
  * (polls of the staging mbarrier; PYST_MBAR_POLL_LIMIT by default).  With
  * 0 every staging wait gives up at once, so a test can see the timeout

@@ -140,6 +140,7 @@ SIGNATURES = {
     'pyst_test_math': (C.c_int, [_p, C.c_int64, C.c_int, _p, _p]),
     'pyst_test_poisson': (C.c_int, [_p, C.c_int64, C.c_uint64, _p, _p]),
     'pyst_test_set_staging_polls': (C.c_int, [C.c_int32]),
+    'pyst_test_model_packable': (C.c_int, [_p]),
     'pyst_test_pipe': (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _p, _p]),
 }
 

@@ -219,6 +219,13 @@ extern "C" {
 
 int pyst_abi_version(void) { return PYST_ABI_VERSION; }
 
+int pyst_test_model_packable(const uint32_t* h_blob) {
+  HostModelInfo mi;
+  const int rc = read_header(h_blob, &mi);
+  if (rc) return -rc;
+  return mi.packable ? 1 : 0;
+}
+
 int pyst_test_set_staging_polls(int32_t polls) {
   return g_stage_polls.exchange(polls < 0 ? PYST_MBAR_POLL_LIMIT : polls);
 }

@@ -218,9 +218,10 @@ __device__ __forceinline__ float propensity(const ModelView& m, int j,
 // < 1024.  The packed forms take the same operations in the same order as
 // the entry lists, so results are identical; they only remove the chains
 // of dependent shared-memory loads (entry pointer -> entry -> species).
-// Whether reaction j of the blob at `w` (header and sections, host or
-// device memory) fits the packed descriptors.  Shared by the device packer
-// and the host launchers, so both decide alike.
+// Whether reaction j of the blob at `w` fits the packed descriptors: the
+// host launchers' form of the conditions pack_reactions checks inline (its
+// own form keeps the mode-sorted kernel's register allocation unchanged);
+// tests check that both decide alike.
 __host__ __device__ inline bool blob_reaction_packable(const uint32_t* w,
                                                        int j) {
   const int ofp = (int)w[PYST_H_OFF_FACPTR], of = (int)w[PYST_H_OFF_FAC];
@@ -243,17 +244,19 @@ __host__ __device__ inline bool blob_reaction_packable(const uint32_t* w,
   return true;
 }
 
-// All threads of the block call this; true when every reaction fits.
+// All threads of the block call this; true when every reaction fits (the
+// conditions of blob_reaction_packable, checked inline).
 __device__ __forceinline__ bool pack_reactions(const ModelView& m,
                                                uint32_t* pk) {
   bool ok = m.nlaw == 0;  // kinetic-law programs use the general path
   for (int j = threadIdx.x; j < m.R; j += blockDim.x) {
-    ok &= blob_reaction_packable(m.w, j);
     const int e0 = m.facptr(j), e1 = m.facptr(j + 1);
     uint32_t d = 0;
+    if (e1 - e0 > 2) ok = false;
     for (int e = e0; e < e1 && e < e0 + 2; ++e) {
       const uint32_t fe = m.fac(e);
       const int sp = ent_lo(fe), n = fac_order(fe);
+      if (sp > 1023 || n < 1 || n > 3) ok = false;
       d |= ((uint32_t)(sp & 1023) | ((uint32_t)(n & 3) << 10) |
             ((uint32_t)fac_falling(fe) << 12))
            << (13 * (e - e0));
@@ -261,9 +264,11 @@ __device__ __forceinline__ bool pack_reactions(const ModelView& m,
     pk[j] = d;
     const int n0 = m.netptr(j), n1 = m.netptr(j + 1);
     uint32_t q = (uint32_t)(n1 - n0) << 30;
+    if (n1 - n0 > 2) ok = false;
     for (int e = n0; e < n1 && e < n0 + 2; ++e) {
       const uint32_t ne = m.net(e);
       const int sp = ent_lo(ne), v = ent_hi_s16(ne);
+      if (sp > 1023 || v < -16 || v > 15) ok = false;
       q |= ((uint32_t)(sp & 1023) | ((uint32_t)(v & 31) << 10))
            << (15 * (e - n0));
     }

@@ -589,7 +589,10 @@ int PYST_CAT(launch_plain_thread_, PYST_TAU, PYST_SCORE)(
   if (maxr > PYST_THREAD_MAX_REACTIONS) return PYST_EUNSUPPORTED;
 #endif
 #if !PYST_TAU && !PYST_SCORE
-  // fewer trajectories than one 128-thread block of lane groups per SM
+  // runs too small to fill the GPU: at most kGroupMaxPerSm trajectories per
+  // SM, each on a whole warp (kGroupLanes = 32 lanes by default) -- the
+  // lane tree for packable models of at most kSpecMaxSpecies species, the
+  // lockstep lane groups otherwise
   if (maxr <= 8 && bs <= 128 && bs % kGroupLanes == 0 &&
       n <= (int64_t)num_sms() * kGroupMaxPerSm) {
     if (PYST_SPEC_TREE && mi.packable && mi.S <= kSpecMaxSpecies)

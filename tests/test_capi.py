@@ -187,3 +187,52 @@ def test_blob_size_query_matches_build(built_lib):
     assert built_lib.pyst_model_build(C.byref(d), buf.ctypes.data,
                                       buf.size) == _lib.PYST_EINVAL
     assert len(m.blob()) == n.value
+
+
+def _packable_py(m):
+    """Restatement of the packing conditions: at most two reactant entries
+    of order 1..3 and two net-change entries with -16 <= delta <= 15, over
+    species < 1024, and no general kinetic laws."""
+    if m.has_laws:
+        return False
+    for j in range(m.n_reactions):
+        fac = [i for i in range(m.n_species) if m.order[i, j] > 0]
+        net = [i for i in range(m.n_species) if m.net[i, j] != 0]
+        if len(fac) > 2 or len(net) > 2:
+            return False
+        if any(m.order[i, j] > 3 or i > 1023 for i in fac):
+            return False
+        if any(not -16 <= m.net[i, j] <= 15 or i > 1023 for i in net):
+            return False
+    return True
+
+
+def test_host_packable_predicate(built_lib):
+    """The host's packability decision (which picks the lane-tree kernel)
+    against a restatement, on models at every boundary."""
+    from py_stoch_b200.model import Model
+    cases = [networks.lotka_volterra(), networks.schlogl(),
+             networks.telegraph(), _law_model()]
+    t = np.linspace(0, 1, 3).astype(np.float32)
+    for delta in (15, 16, -16, -17):
+        pre = [[1], [0]]
+        post = [[1 + delta if delta > 0 else 1], [0]]
+        if delta < 0:
+            pre, post = [[-delta], [0]], [[0], [0]]
+        cases.append(Model.mass_action(pre, post, [1.0], [100, 5], t))
+    for order in (3, 4):
+        cases.append(Model.mass_action([[order]], [[order + 1]], [1.0],
+                                       [50], t))
+    # three reactant species, three net-change species
+    cases.append(Model.mass_action([[1], [1], [1]], [[0], [0], [2]], [1.0],
+                                   [9, 9, 9], t))
+    cases.append(Model.mass_action([[1], [0], [0]], [[0], [1], [1]], [1.0],
+                                   [9, 0, 0], t))
+    cases += networks.synthetic_networks(6, seed=4)
+    seen = set()
+    for m in cases:
+        want = _packable_py(m)
+        seen.add(want)
+        assert built_lib.pyst_test_model_packable(m.blob().ctypes.data) == \
+            int(want), m.name
+    assert seen == {True, False}

@@ -137,11 +137,16 @@ def test_schlogl_direct(torch_cuda, built_lib, oracle_mod, mapping):
     _compare(g, o)
 
 
-@pytest.mark.parametrize('n', [100, 2368, 2369, 4096])
-def test_direct_thread_run_sizes(torch_cuda, built_lib, oracle_mod, n):
-    """Direct-method thread runs on both sides of the lane-group limit
-    (a warp per trajectory up to 148 x 16 trajectories, one thread per
-    trajectory above it, where the runs fill the GPU)."""
+@pytest.mark.parametrize('which', ['small', 'limit', 'limit+1', 'large'])
+def test_direct_thread_run_sizes(torch_cuda, built_lib, oracle_mod, which):
+    """Direct-method thread runs on both sides of the small-run limit: up to
+    16 trajectories per SM (the device's SM count x 16) each trajectory gets
+    a whole warp (the lane tree for packable models), above it one thread
+    per trajectory."""
+    sms = torch_cuda.cuda.get_device_properties(0).multi_processor_count
+    limit = sms * 16
+    n = {'small': 100, 'limit': limit, 'limit+1': limit + 1,
+         'large': limit + 1700}[which]
     m = networks.schlogl(t_end=1.0, n_samples=21)
     g = _gpu(torch_cuda, m, n, 'direct', 'thread', seed=3)
     o = _oracle(oracle_mod, m, n, 'direct', 'thread', seed=3)
@@ -391,3 +396,36 @@ def test_batch_stats_and_jacobian(torch_cuda, built_lib):
         want_v = np.einsum('kfu,uj->kfj', d * d - v[..., None], s) / x.shape[2]
         np.testing.assert_allclose(jac[0], want_m, rtol=1e-8, atol=1e-8)
         np.testing.assert_allclose(jac[1], want_v, rtol=1e-8, atol=1e-6)
+
+
+def test_small_runs_at_the_packing_boundary(torch_cuda, built_lib,
+                                            oracle_mod):
+    """Small direct-method runs (a warp per trajectory) of models on both
+    sides of the packed-descriptor limits: the host picks the lane tree for
+    packable ones and the lockstep lane groups otherwise; both equal the
+    oracle.  Also every lane-tree depth: R = 1 and 2 (5 levels), 3 and 4
+    (3 levels), 5 to 8 (2 levels)."""
+    from py_stoch_b200 import _lib
+    t = np.linspace(0, 0.05, 6).astype(np.float32)
+    models = []
+    for delta in (15, 16):
+        models.append(Model.mass_action([[1], [0]], [[1 + delta], [0]],
+                                        [2.0], [100, 5], t))
+    for order in (3, 4):
+        models.append(Model.mass_action([[order], [0]], [[order - 1], [1]],
+                                        [1e-3], [60, 0], t))
+    models.append(Model.mass_action([[1], [1], [1]], [[0], [0], [2]], [1.0],
+                                    [90, 90, 90], t))
+    for R in (1, 2, 5, 8):
+        models += networks.synthetic_networks(1, seed=40 + R, s_range=(2, 6),
+                                              r_range=(R, R),
+                                              t_range=(0.002, 0.01))
+    kinds = set()
+    for i, m in enumerate(models):
+        kinds.add(built_lib.pyst_test_model_packable(m.blob().ctypes.data))
+        g = _gpu(torch_cuda, m, 64, 'direct', 'thread', seed=i,
+                 step_budget=200000)
+        o = _oracle(oracle_mod, m, 64, 'direct', 'thread', seed=i,
+                    step_budget=200000)
+        _compare(g, o)
+    assert kinds == {0, 1}
