@@ -296,7 +296,7 @@ def batch_vs_plain(kind, dev, subset=256, steps=1, full=True, budget=20000):
     int32 overflows (Lotka-Volterra sets whose prey grows without bound)
     in `status_counts`."""
     import torch
-    from py_stoch_b200 import networks
+    from py_stoch_b200 import _lib, networks
     from py_stoch_b200.autotune import Autotuner
     from py_stoch_b200.batch import Batch
     from py_stoch_b200.simulator import simulate
@@ -325,6 +325,8 @@ def batch_vs_plain(kind, dev, subset=256, steps=1, full=True, budget=20000):
         b = Batch(ms, n_traj, method='tau', mapping_fn=tuner.mapping_fn,
                   device=dev, score=grad, stats=grad, jacobian=grad,
                   traj_id_base=ids)
+        batched_maps['same' if ids is not None else 'full'] = [
+            int(x) for x in b.mappings]
         g = b.graph(seed=11, step_budget=budget)
         g.replay()  # untimed: the first replay after capture ran slower
         clk = ClockSampler(dev.index or 0)
@@ -342,10 +344,11 @@ def batch_vs_plain(kind, dev, subset=256, steps=1, full=True, budget=20000):
                            len(ms), n_traj, 1)
         rec['work_items'] = int(b.n_items)
         rec['clocks'] = clocks
-        return rec
+        return rec, b
 
     ids = [i * n_traj for i in pick]
-    res['batched_same_models'] = batched(sub, ids)
+    batched_maps = {}
+    res['batched_same_models'], sub_batch = batched(sub, ids)
     # plain form: one simulate() launch per model, same ids and budget
     outs = [{'samples': torch.empty((m.kappa, m.ita, n_traj),
                                     dtype=torch.int32, device=dev),
@@ -353,14 +356,20 @@ def batch_vs_plain(kind, dev, subset=256, steps=1, full=True, budget=20000):
              'status': torch.empty(n_traj, dtype=torch.uint8, device=dev)}
             for m in sub]
 
+    # the plain form's mapping per model: what the library picks for one
+    # launch of n_traj trajectories (a warp per trajectory for networks
+    # beyond the register engine's 32 reactions, since such a launch cannot
+    # fill the GPU thread by thread); the batch tuner's choices are for
+    # full batches
+    plain_map = ['warp' if (m.n_reactions > _lib.THREAD_MAX_REACTIONS or
+                            m.n_species > 64) else 'thread' for m in sub]
+
     def plain():
         for k, (m, i) in enumerate(zip(sub, pick)):
             simulate(m, n_traj, method='tau', seed=11,
                      traj_id_base=i * n_traj, device=dev, stream=stream,
                      out=outs[k], score=grad, status=True,
-                     step_budget=budget,
-                     mapping=('thread' if tuner.mapping(m, 'tau') == 1
-                              else 'warp'))
+                     step_budget=budget, mapping=plain_map[k])
     ms_p, _ = _events_timed(plain, stream)
     ev_p = float(sum(int(o['events'].sum().item()) for o in outs))
     ok_p = sum(completed_events(o['events'], o['status']) for o in outs)
@@ -374,10 +383,21 @@ def batch_vs_plain(kind, dev, subset=256, steps=1, full=True, budget=20000):
     res['batched_over_plain_completed'] = (
         bs['completed_events_per_s'] /
         max(res['plain']['completed_events_per_s'], 1e-30))
-    res['same_results'] = bool(bs['events'] == ev_p and bs[
-        'status_counts'] == res['plain']['status_counts'])
+    # identical per-trajectory results where both forms map a model alike
+    # (warp-mapped runs sum propensities in another order)
+    bmaps = batched_maps['same']
+    alike = [k for k in range(len(sub))
+             if (bmaps[k] == _lib.MAP_WARP) == (plain_map[k] == 'warp')]
+    ok = True
+    for k in alike:
+        ok &= bool(torch.equal(outs[k]['events'],
+                               sub_batch.per_traj('events', k)))
+        ok &= bool(torch.equal(outs[k]['samples'], sub_batch.samples(k)))
+    res['same_results'] = {'models_compared': len(alike), 'equal': ok}
+    del sub_batch
     if full:
-        res['batched_full'] = batched(models)
+        res['batched_full'], fb = batched(models)
+        del fb
     res['autotune'] = {k: v['mapping'] for k, v in tuner.table.items()
                        if 'mapping' in v}
     torch.cuda.empty_cache()
@@ -599,6 +619,9 @@ def run_plain(wl, steps, warmup, dev, world=1, rank=0, e2e=True,
          'trajectories_per_s': n * world * steps / (total_ms / 1e3),
          'error_trajectories': int(errs), 'clocks': clocks,
          'status_counts': status_counts.tolist(),
+         # this library's kernels per step: the simulation, plus the
+         # moments (sums, moments) and the two-kernel score reduction of
+         # the gradient form
          'gpu_launches': steps * (5 if grad else 1),
          'out_bytes': sum(v.numel() * v.element_size()
                           for v in out.values())}
@@ -695,7 +718,7 @@ def plain_record(name, wl, args, dev, peaks, steps, warmup, world=1,
     Tau-leaping workloads run with the mode-sorted scheduler geometry the
     autotuner picks for them (measured before the timed region)."""
     geometry = None
-    if wl['method'] == 'tau':
+    if wl['method'] == 'tau' and not args.no_tune:
         from py_stoch_b200.autotune import Autotuner
         geometry = Autotuner(device=dev).tune_geometry(wl['model'], wl['n'],
                                                        'tau')
@@ -726,6 +749,8 @@ def main():
                     help='override trajectories per GPU (profiling runs)')
     ap.add_argument('--no-configs', action='store_true',
                     help='headline only: skip the other configurations')
+    ap.add_argument('--no-tune', action='store_true',
+                    help='default scheduler geometry (profiling runs)')
     args = ap.parse_args()
     if args.workload in ('sweep', 'synthetic'):
         return forms_main(args)

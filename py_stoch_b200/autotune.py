@@ -104,8 +104,12 @@ class Autotuner(object):
         torch = _torch()
         kw = ({'mapping_fn': mapping} if callable(mapping) else
               {'mapping': mapping})
+        # whole models per block (no trajectory chunks): a trial batch is
+        # far smaller than the GPU, and chunks would favour whichever
+        # mapping splits into more blocks, while a full batch fills the GPU
+        # either way and runs at the per-block rate compared here
         b = Batch(models, self.n_traj, method=method, device=self.device,
-                  score=self.score, **kw)
+                  score=self.score, chunk=0, **kw)
         b.run(seed=0x5EED, step_budget=self.budget, block_size=block_size)
         st = torch.cuda.Event(enable_timing=True)
         en = torch.cuda.Event(enable_timing=True)

@@ -20,6 +20,10 @@ from . import _lib
 from .simulator import DEFAULT_STEP_BUDGET, _mapping, _method, _torch
 
 
+# Resident threads per SM of the batched kernel (6 blocks of 128).
+BATCH_THREADS_PER_SM = 768
+
+
 def estimated_cost(model, method):
     """Rough work estimate of one trajectory: total propensity at x0 times
     the simulated time (events for the direct method)."""
@@ -54,7 +58,8 @@ class Batch(object):
     def __init__(self, models, n_traj, method='direct', mapping='auto',
                  traj_id_base=None, device=None, score=False, status=True,
                  events=True, seqhash=False, t_final=False, order='cost',
-                 mapping_fn=None, stats=False, jacobian=False, chunk=128):
+                 mapping_fn=None, stats=False, jacobian=False, chunk=128,
+                 small_batch_warps=True):
         torch = _torch()
         self.device = torch.device(device or 'cuda')
         self.models = list(models)
@@ -85,6 +90,20 @@ class Batch(object):
                     m.n_reactions > _lib.THREAD_MAX_REACTIONS):
                 x = _lib.MAP_WARP
             mp.append(x)
+        # A batch whose trajectories would fill less than half the GPU
+        # thread by thread is latency-bound: networks beyond the register
+        # engine's reactions then run a warp per trajectory (each step's
+        # reactions over 32 lanes), whatever a full-batch tuning chose.
+        chosen_here = mapping_fn is not None or (
+            isinstance(mapping, (str, int)) and
+            _mapping(mapping) == _lib.MAP_AUTO)
+        if small_batch_warps and chosen_here:
+            props = torch.cuda.get_device_properties(self.device)
+            capacity = props.multi_processor_count * BATCH_THREADS_PER_SM
+            if int(self.n_traj.sum()) * 2 < capacity:
+                mp = [_lib.MAP_WARP if (m.n_reactions >
+                                        _lib.THREAD_MAX_REACTIONS) else x
+                      for m, x in zip(self.models, mp)]
         self.mappings = np.array(mp, np.int32)
         if traj_id_base is None:
             traj_id_base = np.concatenate([[0], np.cumsum(self.n_traj)[:-1]])

@@ -45,6 +45,9 @@ namespace {
 #define PYST_CAP_LEAP 3
 #endif
 constexpr int kSortedCapSsa = PYST_CAP_SSA;
+// Auto mapping of networks with more reactions than the register engine:
+// warps when the run has at most this many trajectories per SM.
+constexpr int kWarpAutoPerSm = 32;
 constexpr int kSortedCapLeap = PYST_CAP_LEAP;
 
 // The factor and net-change sections of a host blob lie inside it (so the
@@ -163,8 +166,14 @@ int single_run(const uint32_t* h_blob, const uint32_t* d_blob,
   const bool score = out->score != nullptr;
   int mapping = run->mapping;
   const int bs = run->block_size ? run->block_size : 128;
+  // auto: a thread per trajectory unless the species columns are large,
+  // the scores' register accumulators do not fit, or a run of a large
+  // network is too small to fill the GPU (a warp then spreads each step's
+  // reactions over 32 lanes instead of looping over them in one thread)
   if (mapping == PYST_MAP_AUTO)
-    mapping = (mi.S <= 64 && (mi.R <= PYST_THREAD_MAX_REACTIONS || !score))
+    mapping = (mi.S <= 64 && (mi.R <= PYST_THREAD_MAX_REACTIONS ||
+                              (!score && run->n_traj > (int64_t)num_sms() *
+                                                           kWarpAutoPerSm)))
                   ? PYST_MAP_THREAD
                   : PYST_MAP_WARP;
   // thread-mapped scores keep per-reaction accumulators in registers

@@ -818,8 +818,10 @@ __device__ void thread_finish(const ModelView& m, const int32_t* xcol, int bs,
   }
 }
 
-// One whole trajectory by the calling thread.
-template <int MAXR, bool TAU, bool SCORE>
+// One whole trajectory by the calling thread.  PK: kPkPacked or kPkLists
+// when the caller knows the form (the host checks packability), -1 to
+// choose by m.fast at run time (batched launches mix models).
+template <int MAXR, bool TAU, bool SCORE, int PK = -1>
 __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
                            int bs, const RunArgs& ra, uint64_t traj_id,
                            const TrajOut& o) {
@@ -832,11 +834,11 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
     integ[j] = 0.0;
     cnt[j] = 0;
   }
-  if (m.fast)
+  if (PK == kPkPacked || (PK < 0 && m.fast))
     thread_round<MAXR, TAU, SCORE, kPkPacked>(m, xcol, slot, bs, bs, ra,
                                               traj_id, st, integ, cnt, o,
                                               0x7fffffff, 0x7fffffff, false);
-  else
+  else if (PK == kPkLists || PK < 0)
     thread_round<MAXR, TAU, SCORE, kPkLists>(m, xcol, slot, bs, bs, ra,
                                              traj_id, st, integ, cnt, o,
                                              0x7fffffff, 0x7fffffff, false);
@@ -1129,8 +1131,9 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
 #undef SL
 }
 
-// thread_round for MAXR > 0 (register arrays), thread_round_big for 0
-template <int MAXR, bool TAU, bool SCORE>
+// thread_round for MAXR > 0 (register arrays), thread_round_big for 0; PK
+// as thread_round's (kPkPacked when the caller knows every reaction packs)
+template <int MAXR, bool TAU, bool SCORE, int PK = kPkRuntime>
 __device__ __forceinline__ void any_round(
     const ModelView& m, int32_t* xcol, int64_t* slot, int bs, int ss,
     const RunArgs& ra, uint64_t traj_id, TState& st, double* integ, int* cnt,
@@ -1140,10 +1143,9 @@ __device__ __forceinline__ void any_round(
     thread_round_big<TAU>(m, xcol, slot, bs, ss, ra, traj_id, st, o, cap_ssa,
                           cap_leap, stop_on_switch);
   } else {
-    thread_round<MAXR, TAU, SCORE, kPkRuntime>(m, xcol, slot, bs, ss, ra,
-                                               traj_id, st, integ, cnt, o,
-                                               cap_ssa, cap_leap,
-                                               stop_on_switch);
+    thread_round<MAXR, TAU, SCORE, PK>(m, xcol, slot, bs, ss, ra, traj_id,
+                                       st, integ, cnt, o, cap_ssa, cap_leap,
+                                       stop_on_switch);
   }
 }
 

@@ -182,8 +182,10 @@ __device__ __forceinline__ void fill_slot(const SortedSmem& s,
   }
 }
 
-// NB: block size fixed at compile time, or 0 for blockDim.x.
-template <int MAXR, int NB>
+// NB: block size fixed at compile time, or 0 for blockDim.x.  PK:
+// kPkPacked for models whose every reaction packs (the host checks), else
+// kPkRuntime.
+template <int MAXR, int NB, int PK>
 __global__ void __launch_bounds__(kMaxBlock, kMinBlocks)
     k_tau_sorted(const uint32_t* __restrict__ gblob, int blob_words,
                  int64_t n_traj, uint64_t id_base, RunArgs ra, OutBase ob,
@@ -329,10 +331,10 @@ __global__ void __launch_bounds__(kMaxBlock, kMinBlocks)
       }
       const int64_t u = sm.traj[p];
       const TrajOut o = ob.at(0, u, 0, 0, ob.stride, R);
-      any_round<MAXR, true, kScore>(m, sm.x + p, sm.scratch + tid, slots,
-                                    nb, ra, id_base + (uint64_t)u, st,
-                                    integ, cnt, o, my_cap_ssa, my_cap_leap,
-                                    true);
+      any_round<MAXR, true, kScore, PK>(m, sm.x + p, sm.scratch + tid,
+                                        slots, nb, ra, id_base + (uint64_t)u,
+                                        st, integ, cnt, o, my_cap_ssa,
+                                        my_cap_leap, true);
       if (st.flags & TS_DONE) {
         thread_finish<(MAXR > 0 ? MAXR : 1), kScore>(m, sm.x + p, slots, st,
                                                      integ, cnt, o);
@@ -378,8 +380,13 @@ int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
       }
   if (!block) return PYST_EUNSUPPORTED;
   const size_t smem = sorted_smem_bytes(mi.words, mi.S, maxr, pool, block);
-  auto kf = block == kMaxBlock ? k_tau_sorted<MR, kMaxBlock>
-                               : k_tau_sorted<MR, 0>;
+  // compile-time packed descriptors when every reaction packs (MAXR > 0)
+  constexpr int kPk = MR > 0 ? kPkPacked : kPkRuntime;
+  auto kf = mi.packable
+                ? (block == kMaxBlock ? k_tau_sorted<MR, kMaxBlock, kPk>
+                                      : k_tau_sorted<MR, 0, kPk>)
+                : (block == kMaxBlock ? k_tau_sorted<MR, kMaxBlock, kPkRuntime>
+                                      : k_tau_sorted<MR, 0, kPkRuntime>);
   const int rc = set_smem(kf, smem);
   if (rc) return rc;
   if (cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st) !=

@@ -27,7 +27,9 @@ namespace PYST_CAT(thread_flavour_, PYST_TAU, PYST_SCORE) {
 #define PYST_THREAD_MINB 6
 #endif
 
-template <int MAXR, bool TAU, bool SCORE>
+// PK: kPkPacked for models whose every reaction packs (the host checks),
+// kPkLists otherwise (general kinetic laws included).
+template <int MAXR, bool TAU, bool SCORE, int PK>
 __global__ void __launch_bounds__(128, PYST_THREAD_MINB)
     k_plain_thread(const uint32_t* __restrict__ gblob, int blob_words,
                    int64_t n_traj, uint64_t id_base, RunArgs ra, OutBase ob,
@@ -74,8 +76,8 @@ __global__ void __launch_bounds__(128, PYST_THREAD_MINB)
     if constexpr (MAXR == 0)
       run_thread_big<TAU>(m, xcol, slot, bs, ra, id_base + (uint64_t)u, o);
     else
-      run_thread<MAXR, TAU, SCORE>(m, xcol, slot, bs, ra,
-                                   id_base + (uint64_t)u, o);
+      run_thread<MAXR, TAU, SCORE, PK>(m, xcol, slot, bs, ra,
+                                       id_base + (uint64_t)u, o);
     u = nthreads + (int64_t)atomicAdd(queue, 1ull);
   }
 }
@@ -110,9 +112,12 @@ constexpr int kGroupMaxPerSm = 16;
 // j_1 .. j_d, computes its propensities, total, tau and selection for step
 // d + 1 (with step d + 1's random numbers), and a few ballots publish every
 // lane's selection, so each lane walks the tree from the root along the
-// selections to the true path.  Lanes per depth grow as R^d, so the depth
-// D is 5 for R <= 2 (31 lanes), 3 for R <= 4 (21) and 2 for R <= 8 (9):
-// Lotka-Volterra (R = 3) advances 3 steps per pass on 13 lanes.
+// selections to the true path.  Lanes per depth grow as R^d, so the full
+// depth D is 5 for R <= 2 (31 lanes), 3 for R <= 4 (21) and 2 for R <= 8
+// (9); the lanes left over cover part of level D, so a pass whose true
+// path is there takes one step more: Lotka-Volterra (R = 3) advances 3
+// steps per pass on 13 lanes, or 4 when its path is among the 19 of 27
+// covered at level 3.
 // The passes commit only when none of the D steps reaches a sample time,
 // absorbs, runs out of step budget or leaves the int32 range; otherwise D
 // exact single steps run instead (thread_round's order of operations, which
@@ -210,6 +215,13 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
   const int lane = threadIdx.x & 31;
   // this lane's depth dl and path j_1 .. j_dl (base-R digits of its index
   // within the depth, first firing first)
+  // Full levels 0 .. D-1 take `used` lanes; the remaining lanes cover the
+  // first `extra` paths of level D, so a pass whose true path is among
+  // them commits D + 1 steps.
+  const int used = spec_lanes(R, D);
+  int width_d = 1;
+  for (int d = 0; d < D; ++d) width_d *= R;
+  const int extra = 32 - used < width_d ? 32 - used : width_d;
   int dl = 0, il = 0;
   {
     int st = 0, w = 1;
@@ -222,8 +234,12 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
       st += w;
       w *= R;
     }
+    if (lane >= used && lane < used + extra) {
+      dl = D;
+      il = lane - used;
+    }
   }
-  const bool in_tree = lane < spec_lanes(R, D);
+  const bool in_tree = lane < used + extra;
   // the path's net change, and the extremes of its running sum, per species
   // (the states along the path stay in [0, 2^31) iff x + lo >= 0 and
   // x + hi < 2^31), fixed for the whole trajectory
@@ -309,16 +325,18 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
       const int sel = select_reaction<MAXR>(a, R, __dmul_rn(u, a0));
       ok &= a0 != 0.0;
       // the state after this lane's step (needed from the deepest lane of
-      // the true path): its range check joins the lane's flag
-      if (dl == D - 1) ok &= reg_apply(xs, m.pk[R + (sel < 0 ? 0 : sel)]);
+      // the true path, at level D - 1 or D): its range check joins the
+      // lane's flag
+      if (dl >= D - 1) ok &= reg_apply(xs, m.pk[R + (sel < 0 ? 0 : sel)]);
       unsigned sb[kSelBits];
 #pragma unroll
       for (int b = 0; b < kSelBits; ++b)
         sb[b] = __ballot_sync(0xffffffffu, (sel >> b) & 1);
       const unsigned bad = __ballot_sync(0xffffffffu, !ok);
       // ---- walk the tree along the selections (uniform) ---------------
-      int J[D], L[D];
+      int J[D + 1], L[D + 1];
       unsigned badpath = 0u;
+      int dn = D;  // steps this pass commits
       {
         int i = 0, st = 0, w = 1;
 #pragma unroll
@@ -335,21 +353,39 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
           st += w;
           w *= R;
         }
+        // one step more when the partial level holds the path, its step
+        // is sound and within the budget (otherwise the next pass or the
+        // exact steps take it)
+        const int ln = used + i;
+        L[D] = ln;
+        J[D] = 0;
+        if (i < extra && !((bad >> ln) & 1u) && steps + D + 1 <= budget) {
+          int j = 0;
+#pragma unroll
+          for (int b = 0; b < kSelBits; ++b)
+            j |= (int)((sb[b] >> ln) & 1u) << b;
+          J[D] = j;
+          dn = D + 1;
+        }
       }
       if (!badpath) {
         double tt = t;
 #pragma unroll
-        for (int d = 0; d < D; ++d)
-          tt = __dadd_rn(tt, __shfl_sync(0xffffffffu, tau, L[d]));
+        for (int d = 0; d <= D; ++d) {
+          const double td = __shfl_sync(0xffffffffu, tau, L[d]);
+          if (d < dn) tt = __dadd_rn(tt, td);
+        }
         if (tt < tf) {
+          const int last = dn > D ? L[D] : L[D - 1];
 #pragma unroll
           for (int s = 0; s < MAXS; ++s)
-            x[s] = __shfl_sync(0xffffffffu, xs[s], L[D - 1]);
+            x[s] = __shfl_sync(0xffffffffu, xs[s], last);
 #pragma unroll
-          for (int d = 0; d < D; ++d) h = seq_mix(h, (uint64_t)J[d]);
+          for (int d = 0; d <= D; ++d)
+            if (d < dn) h = seq_mix(h, (uint64_t)J[d]);
           t = tt;
-          steps += D;
-          events += D;
+          steps += dn;
+          events += dn;
           committed = true;
         }
       }
@@ -552,7 +588,12 @@ template <int MR>
 int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
                uint64_t id_base, const RunArgs& ra, const OutBase& ob, int bs,
                cudaStream_t st, size_t smem, unsigned long long* queue) {
-  auto kf = k_plain_thread<MR, (bool)PYST_TAU, (bool)PYST_SCORE>;
+  // the packed-descriptor form compiled on its own for packable models
+  auto kf = (MR > 0 && mi.packable)
+                ? k_plain_thread<MR, (bool)PYST_TAU, (bool)PYST_SCORE,
+                                 kPkPacked>
+                : k_plain_thread<MR, (bool)PYST_TAU, (bool)PYST_SCORE,
+                                 kPkLists>;
   const int rc = set_smem(kf, smem);
   if (rc) return rc;
   int per_sm = 1;

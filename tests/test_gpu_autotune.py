@@ -65,17 +65,26 @@ def test_tune_mixed_buckets_cache_and_parity(torch_cuda, built_lib,
     bs = tuner.tune_block(models, 'tau')
     assert bs in (64, 128)
     budget = 100000
-    b = Batch(models, 48, method='tau', mapping_fn=tuner.mapping_fn)
+    b = Batch(models, 48, method='tau', mapping_fn=tuner.mapping_fn,
+              small_batch_warps=False)
     b.run(seed=31, step_budget=budget, block_size=bs)
     assert list(b.mappings) == [tuner.mapping(m, 'tau') for m in models]
     _check_batch(torch_cuda, oracle_mod, b, models, 48, budget)
     # force one bucket to the warp mapping through the cache
     k = bucket(models[0], 'tau')
     again.table[k] = dict(again.table[k], mapping='warp')
-    b2 = Batch(models, 48, method='tau', mapping_fn=again.mapping_fn)
+    b2 = Batch(models, 48, method='tau', mapping_fn=again.mapping_fn,
+               small_batch_warps=False)
     assert int(b2.mappings[0]) == _lib.MAP_WARP
     b2.run(seed=31, step_budget=budget)
     _check_batch(torch_cuda, oracle_mod, b2, models, 48, budget)
+    # a batch too small to fill the GPU runs its large networks warp-mapped
+    b3 = Batch(models, 48, method='tau', mapping_fn=tuner.mapping_fn)
+    assert [int(x) == _lib.MAP_WARP for x in b3.mappings] == [
+        m.n_reactions > _lib.THREAD_MAX_REACTIONS or
+        tuner.mapping(m, 'tau') == _lib.MAP_WARP for m in models]
+    b3.run(seed=31, step_budget=budget)
+    _check_batch(torch_cuda, oracle_mod, b3, models, 48, budget)
 
 
 def test_sorted_geometry_search(torch_cuda, built_lib, oracle_mod, tmp_path):
