@@ -50,17 +50,14 @@ def workloads():
             # from one ncu capture of the simulation kernel on 229,376
             # trajectories: DRAM read + write per trajectory, and warp
             # instructions per reaction event
-            dram_bytes_per_traj=(519.8e6 + 1382.3e6) / 229376,
-            warp_inst_per_event=41112782222 / 4209068063),
+            dram_bytes_per_traj=(609.38e6 + 1625.83e6) / 229376,
+            warp_inst_per_event=39590902418 / 4209068063),
         'lv_ssa': dict(
             model=networks.lotka_volterra(), n=1024, method='direct',
             desc='plain Gillespie direct method, Lotka-Volterra (k1=10, '
                  'k2=0.01, k3=10), X0=Y0=1000, 1024 trajectories, t_end=10,'
                  ' 100 samples, Philox ids 0..1023',
-            cpu_pilot=64, ref_config='lv_ssa_1024',
-            # warp instructions per reaction event of the lane-group
-            # kernel, from one ncu capture of this workload
-            warp_inst_per_event=64533376180 / 307266234),
+            cpu_pilot=64, ref_config='lv_ssa_1024'),
         'telegraph_grad': dict(
             model=networks.telegraph(), n=1048576, method='direct', grad=True,
             desc='adjoint gradient: telegraph gene expression (k_on=0.5, '
