@@ -27,6 +27,7 @@ namespace PYST_CAT(thread_flavour_, PYST_TAU, PYST_SCORE) {
 #define PYST_THREAD_MINB 6
 #endif
 
+
 // PK: kPkPacked for models whose every reaction packs (the host checks),
 // kPkLists otherwise (general kinetic laws included).
 template <int MAXR, bool TAU, bool SCORE, int PK>
@@ -82,49 +83,12 @@ __global__ void __launch_bounds__(128, PYST_THREAD_MINB)
   }
 }
 
-#if !PYST_TAU && !PYST_SCORE
-// Lane groups for runs too small to fill the GPU (direct method): each
-// trajectory is a long dependent chain of steps, so with at most a few
-// warps per SM the step latency, not issue throughput, sets the time.
-// kGroupLanes lanes share one trajectory (thread_round's LG form), which
-// takes the Philox and log work of the other steps off each step's chain.
-// Trajectory u is group u (static assignment); lane 0 of a group writes.
-// A whole warp per trajectory measured fastest (Lotka-Volterra, 1024
-// trajectories: 206.7 ms at 32 lanes, 217.1 at 16, 236.1 at 8): the warp
-// then never diverges between trajectories.
-#ifndef PYST_GROUP_LANES
-#define PYST_GROUP_LANES 32
-#endif
-constexpr int kGroupLanes = PYST_GROUP_LANES;
-// 0 keeps the lane groups on the plain lockstep loop (no lane tree)
-#ifndef PYST_SPEC_TREE
-#define PYST_SPEC_TREE 1
-#endif
-// runs of at most this many trajectories per SM take the lane groups
-constexpr int kGroupMaxPerSm = 16;
-
 // ---------------------------------------------------------------------
-// Speculative lane tree (the lane groups' fast path for small mass-action
-// models).  A step's selection j depends on the state, which depends on the
-// previous selection: one dependent chain per trajectory.  Here the 32
-// lanes of the trajectory's warp evaluate the next D steps at once: the
-// lane at depth d with path (j_1 .. j_d) takes the state after firing
-// j_1 .. j_d, computes its propensities, total, tau and selection for step
-// d + 1 (with step d + 1's random numbers), and a few ballots publish every
-// lane's selection, so each lane walks the tree from the root along the
-// selections to the true path.  Lanes per depth grow as R^d, so the full
-// depth D is 5 for R <= 2 (31 lanes), 3 for R <= 4 (21) and 2 for R <= 8
-// (9); the lanes left over cover part of level D, so a pass whose true
-// path is there takes one step more: Lotka-Volterra (R = 3) advances 3
-// steps per pass on 13 lanes, or 4 when its path is among the 19 of 27
-// covered at level 3.
-// The passes commit only when none of the D steps reaches a sample time,
-// absorbs, runs out of step budget or leaves the int32 range; otherwise D
-// exact single steps run instead (thread_round's order of operations, which
-// handles every such case).  Every lane does exactly the arithmetic of the
-// step it evaluates, so results are those of one thread per trajectory,
-// bit for bit.  Species counts (at most MAXS) live in registers, read and
-// written by unrolled selects.
+// Species counts in registers (at most MAXS), read and written by
+// unrolled selects: the lane tree's state.  (A one-thread-per-trajectory
+// direct-method kernel with species in registers measured slower than the
+// shared-memory columns of k_plain_thread: telegraph, 1M trajectories,
+// 175 vs 165 ms -- the selects cost more than the load they replace.)
 template <int MAXS>
 __device__ __forceinline__ int reg_get(const int (&x)[MAXS], int sp) {
   int v = x[0];
@@ -200,6 +164,49 @@ __device__ __forceinline__ void step_variates(Stream& rs, uint64_t blk,
   u = u53(w.z, w.w);
 }
 
+#if !PYST_TAU && !PYST_SCORE
+// Lane groups for runs too small to fill the GPU (direct method): each
+// trajectory is a long dependent chain of steps, so with at most a few
+// warps per SM the step latency, not issue throughput, sets the time.
+// kGroupLanes lanes share one trajectory (thread_round's LG form), which
+// takes the Philox and log work of the other steps off each step's chain.
+// Trajectory u is group u (static assignment); lane 0 of a group writes.
+// A whole warp per trajectory measured fastest (Lotka-Volterra, 1024
+// trajectories: 206.7 ms at 32 lanes, 217.1 at 16, 236.1 at 8): the warp
+// then never diverges between trajectories.
+#ifndef PYST_GROUP_LANES
+#define PYST_GROUP_LANES 32
+#endif
+constexpr int kGroupLanes = PYST_GROUP_LANES;
+// 0 keeps the lane groups on the plain lockstep loop (no lane tree)
+#ifndef PYST_SPEC_TREE
+#define PYST_SPEC_TREE 1
+#endif
+// runs of at most this many trajectories per SM take the lane groups
+constexpr int kGroupMaxPerSm = 16;
+
+// ---------------------------------------------------------------------
+// Speculative lane tree (the lane groups' fast path for small mass-action
+// models).  A step's selection j depends on the state, which depends on the
+// previous selection: one dependent chain per trajectory.  Here the 32
+// lanes of the trajectory's warp evaluate the next D steps at once: the
+// lane at depth d with path (j_1 .. j_d) takes the state after firing
+// j_1 .. j_d, computes its propensities, total, tau and selection for step
+// d + 1 (with step d + 1's random numbers), and a few ballots publish every
+// lane's selection, so each lane walks the tree from the root along the
+// selections to the true path.  Lanes per depth grow as R^d, so the full
+// depth D is 5 for R <= 2 (31 lanes), 3 for R <= 4 (21) and 2 for R <= 8
+// (9); the lanes left over cover part of level D, so a pass whose true
+// path is there takes one step more: Lotka-Volterra (R = 3) advances 3
+// steps per pass on 13 lanes, or 4 when its path is among the 19 of 27
+// covered at level 3.
+// The passes commit only when none of the D steps reaches a sample time,
+// absorbs, runs out of step budget or leaves the int32 range; otherwise D
+// exact single steps run instead (thread_round's order of operations, which
+// handles every such case).  Every lane does exactly the arithmetic of the
+// step it evaluates, so results are those of one thread per trajectory,
+// bit for bit.  Species counts (at most MAXS) live in registers, read and
+// written by unrolled selects.
 // Lanes of a D-level tree for R reactions: 1 + R + ... + R^(D-1).
 __host__ __device__ constexpr int spec_lanes(int R, int D) {
   return D <= 0 ? 0 : 1 + R * spec_lanes(R, D - 1);
