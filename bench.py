@@ -565,10 +565,10 @@ def run_plain(wl, steps, warmup, dev, world=1, rank=0, e2e=True,
                                    device=dev)
         ones = torch.ones((m.kappa, m.ita), dtype=torch.float64, device=dev)
 
-    def step(seed, d_blob=None):
+    def step(seed, d_blob=None, outs=None):
         res = simulate(m, n, method=meth, seed=seed, traj_id_base=base,
-                       device=dev, stream=stream, out=out, score=grad,
-                       d_blob=d_blob, geometry=geometry)
+                       device=dev, stream=stream, out=outs or out,
+                       score=grad, d_blob=d_blob, geometry=geometry)
         if grad:
             # backward of mean + var of every sample: the score reduction
             mean, var = _moments(res['samples'])
@@ -624,32 +624,57 @@ def run_plain(wl, steps, warmup, dev, world=1, rank=0, e2e=True,
                           for v in out.values())}
     if not e2e:
         return r
-    # end to end through the public API: pinned host model blob in, samples
-    # and per-trajectory status/events (and the gradient) out, every step
+    # End to end through the public API, as an application pipelines it:
+    # every step copies the model blob in from pinned host memory and all
+    # its outputs (samples, status, event counts; the gradient) back to
+    # pinned host memory; outputs are double-buffered and each step's copy
+    # back runs on a copy stream while the next step computes.  One timed
+    # region over all steps, from the first copy in to the last copy out.
     blob = torch.from_numpy(m.blob().view(np.int32)).pin_memory()
     d_blob = torch.empty_like(blob, device=dev)
-    h_out = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
-             for k, v in out.items()}
-    h_grad = torch.empty(m.n_reactions, dtype=torch.float64,
-                         pin_memory=True)
-    e2e_ms, e2e_ev = 0.0, 0
+    bufs = [out, {k: torch.empty_like(v) for k, v in out.items()}]
+    h_bufs = [{k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+               for k, v in out.items()} for _ in range(2)]
+    h_grads = [torch.empty(m.n_reactions, dtype=torch.float64,
+                           pin_memory=True) for _ in range(2)]
+    xstream = torch.cuda.Stream(dev)
+    copied = [None, None]
+    ev_acc = torch.zeros((), dtype=torch.int64, device=dev)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    st = torch.cuda.Event(enable_timing=True)
+    en = torch.cuda.Event(enable_timing=True)
     seed = None
+    st.record(stream)
     for s in range(steps):
+        b = s & 1
         flush.fill_(s & 0xFF)
-        st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(
-            enable_timing=True)
+        if copied[b] is not None:  # buffer b's previous copy is out
+            stream.wait_event(copied[b])
         seed = 100 + s
-        st.record(stream)
         d_blob.copy_(blob, non_blocking=True)
-        res = step(seed, d_blob=d_blob)
-        for k in h_out:
-            h_out[k].copy_(out[k], non_blocking=True)
-        if grad:
-            h_grad.copy_(res['grad'], non_blocking=True)
-        en.record(stream)
-        en.synchronize()
-        e2e_ms += st.elapsed_time(en)
-        e2e_ev += int(h_out['events'].sum())
+        res = step(seed, d_blob=d_blob, outs=bufs[b])
+        ev_acc += bufs[b]['events'].sum()
+        done = torch.cuda.Event()
+        done.record(stream)
+        xstream.wait_event(done)
+        with torch.cuda.stream(xstream):
+            for k in h_bufs[b]:
+                h_bufs[b][k].copy_(bufs[b][k], non_blocking=True)
+            if grad:
+                # (the gradient tensor is read on the copy stream: keep the
+                # allocator from reusing it before that copy is done)
+                res['grad'].record_stream(xstream)
+                h_grads[b].copy_(res['grad'], non_blocking=True)
+        copied[b] = torch.cuda.Event()
+        copied[b].record(xstream)
+    stream.wait_stream(xstream)
+    en.record(stream)
+    en.synchronize()
+    e2e_ms, e2e_ev = st.elapsed_time(en), int(ev_acc.item())
+    h_out = h_bufs[(steps - 1) & 1]
+    h_grad = h_grads[0]
     e2 = torch.tensor([e2e_ms, float(e2e_ev)], dtype=torch.float64,
                       device=dev)
     if world > 1:
@@ -661,7 +686,11 @@ def run_plain(wl, steps, warmup, dev, world=1, rank=0, e2e=True,
     r['e2e'] = {'value': float(e2[1]) / (float(e2[0]) / 1e3), 'unit': UNIT,
                 'h2d_bytes_per_step': blob.numel() * 4,
                 'd2h_bytes_per_step': d2h + (h_grad.numel() * 8 if grad
-                                             else 0)}
+                                             else 0),
+                'ms_per_step': float(e2[0]) / steps,
+                'pipelined': 'outputs double-buffered; each step copied '
+                             'back on a copy stream while the next step '
+                             'computes; one timed region over all steps'}
     # the last end-to-end step's host outputs, for the CPU check
     r['_last'] = {'seed': seed, 'base': base, 'samples':
                   h_out['samples'].numpy(), 'events':

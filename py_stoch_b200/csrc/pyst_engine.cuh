@@ -375,8 +375,15 @@ __device__ __forceinline__ void thread_init(const ModelView& m, int32_t* xcol,
 // numbers, and so the trajectory, are those of LG = 1; only the Philox and
 // log work leaves the per-step dependent chain.  The caller lets one lane
 // of the group write the outputs.
+// GROUP (tau-leaping with stop_on_switch, the mode-sorted scheduler): 0
+// any round; kGroupSsa / kGroupLeap when the caller knows the slot's group,
+// which lets the compiler drop the code such a round never reaches (an SSA
+// round stops when a DECIDE picks a leap, a leap round when it picks SSA
+// steps) -- the same arithmetic, a smaller instruction footprint per warp.
 enum { kPkLists = 0, kPkPacked = 1, kPkRuntime = 2 };
-template <int MAXR, bool TAU, bool SCORE, int PK, int LG = 1>
+enum { kGroupAny = 0, kGroupSsa = 1, kGroupLeap = 2 };
+template <int MAXR, bool TAU, bool SCORE, int PK, int LG = 1,
+          int GROUP = kGroupAny>
 __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
                              int bs, int ss, const RunArgs& ra,
                              uint64_t traj_id, TState& st, double* integ,
@@ -425,8 +432,12 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
   const int64_t budget = ra.step_budget;
   const double t_end = m.time(ita - 1);
   double tf = m.time(f);  // next sample time (f < ita while running)
-  bool ssa_mode = (st.flags & TS_SSA) != 0;
-  const bool group_leap = (st.flags & TS_LEAPGRP) != 0;
+  static_assert(GROUP == kGroupAny || TAU, "groups: tau-leaping only");
+  // (a leap-group slot enters in DECIDE mode: the DECIDE that put it there
+  // picked a leap)
+  bool ssa_mode = GROUP == kGroupLeap ? false : (st.flags & TS_SSA) != 0;
+  const bool group_leap = GROUP == kGroupAny ? (st.flags & TS_LEAPGRP) != 0
+                                             : GROUP == kGroupLeap;
   bool leap_grp = group_leap;
   int ssa_left = st.ssa_left;
   uint32_t leap_q = st.leap_q;
@@ -468,7 +479,7 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
       done = true;
       break;
     }
-    if (TAU && !ssa_mode) {
+    if (TAU && (GROUP == kGroupLeap || !ssa_mode)) {
       // ---------------- DECIDE: critical set, tau_1, SSA switch -------
       uint32_t crit = 0u;
 #pragma unroll
@@ -530,11 +541,12 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
         ssa_mode = true;
         ssa_left = ra.ssa_fallback_steps;
         leap_grp = false;
-        if (stop_on_switch && group_leap) break;  // regroup before stepping
+        // regroup before stepping
+        if (GROUP == kGroupLeap || (stop_on_switch && group_leap)) break;
         // fall through to the SSA step below with the same propensities
       } else {
         leap_grp = true;
-        if (stop_on_switch && !group_leap) break;
+        if (GROUP == kGroupSsa || (stop_on_switch && !group_leap)) break;
         // ---------------- leap ---------------------------------------
         steps++;
         n_leap++;
@@ -1132,8 +1144,9 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
 }
 
 // thread_round for MAXR > 0 (register arrays), thread_round_big for 0; PK
-// as thread_round's (kPkPacked when the caller knows every reaction packs)
-template <int MAXR, bool TAU, bool SCORE, int PK = kPkRuntime>
+// and GROUP as thread_round's
+template <int MAXR, bool TAU, bool SCORE, int PK = kPkRuntime,
+          int GROUP = kGroupAny>
 __device__ __forceinline__ void any_round(
     const ModelView& m, int32_t* xcol, int64_t* slot, int bs, int ss,
     const RunArgs& ra, uint64_t traj_id, TState& st, double* integ, int* cnt,
@@ -1143,9 +1156,10 @@ __device__ __forceinline__ void any_round(
     thread_round_big<TAU>(m, xcol, slot, bs, ss, ra, traj_id, st, o, cap_ssa,
                           cap_leap, stop_on_switch);
   } else {
-    thread_round<MAXR, TAU, SCORE, PK>(m, xcol, slot, bs, ss, ra, traj_id,
-                                       st, integ, cnt, o, cap_ssa, cap_leap,
-                                       stop_on_switch);
+    thread_round<MAXR, TAU, SCORE, PK, 1, GROUP>(m, xcol, slot, bs, ss, ra,
+                                                 traj_id, st, integ, cnt, o,
+                                                 cap_ssa, cap_leap,
+                                                 stop_on_switch);
   }
 }
 

@@ -331,10 +331,18 @@ __global__ void __launch_bounds__(kMaxBlock, kMinBlocks)
       }
       const int64_t u = sm.traj[p];
       const TrajOut o = ob.at(0, u, 0, 0, ob.stride, R);
-      any_round<MAXR, true, kScore, PK>(m, sm.x + p, sm.scratch + tid,
-                                        slots, nb, ra, id_base + (uint64_t)u,
-                                        st, integ, cnt, o, my_cap_ssa,
-                                        my_cap_leap, true);
+      // each round's code for the slot's group only (warps are uniform
+      // but for the one mixed warp, which diverges across the two calls)
+      if (st.flags & TS_LEAPGRP)
+        any_round<MAXR, true, kScore, PK, kGroupLeap>(
+            m, sm.x + p, sm.scratch + tid, slots, nb, ra,
+            id_base + (uint64_t)u, st, integ, cnt, o, my_cap_ssa,
+            my_cap_leap, true);
+      else
+        any_round<MAXR, true, kScore, PK, kGroupSsa>(
+            m, sm.x + p, sm.scratch + tid, slots, nb, ra,
+            id_base + (uint64_t)u, st, integ, cnt, o, my_cap_ssa,
+            my_cap_leap, true);
       if (st.flags & TS_DONE) {
         thread_finish<(MAXR > 0 ? MAXR : 1), kScore>(m, sm.x + p, slots, st,
                                                      integ, cnt, o);
