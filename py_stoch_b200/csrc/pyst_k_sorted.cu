@@ -50,6 +50,8 @@ constexpr int kMinBlocks = kScore ? 4 : 1;
 #define PYST_MIXED_HALF 1
 #endif
 constexpr int kMaxPool = PYST_SORTED_POOL;
+static_assert(kMaxPool <= 2,
+              "the schedule's scan holds at most 64 slot groups");
 constexpr int kPrefBlock =
     PYST_SORTED_BLOCK < kMaxBlock ? PYST_SORTED_BLOCK : kMaxBlock;
 
@@ -261,18 +263,39 @@ __global__ void __launch_bounds__(kMaxBlock, kMinBlocks)
     }
     __syncthreads();
     int tot0 = 0, tot1 = 0, pre0[kMaxPool], pre1[kMaxPool];
+    {
+      // every warp scans the groups' counts itself: lane l holds groups l
+      // and l + 32, the SSA count in the low and the leaping count in the
+      // high 16 bits (a block's slots, at most 2048, fit either half)
+      const int ga = lane, gb = lane + 32;
+      const int ca = ga < groups ? sm.gcnt[ga] | sm.gcnt[groups + ga] << 16
+                                 : 0;
+      const int cb = gb < groups ? sm.gcnt[gb] | sm.gcnt[groups + gb] << 16
+                                 : 0;
+      int va = ca, vb = cb;
 #pragma unroll
-    for (int k = 0; k < kMaxPool; ++k) pre0[k] = pre1[k] = 0;
-    for (int g = 0; g < groups; ++g) {
-#pragma unroll
-      for (int k = 0; k < kMaxPool; ++k) {
-        if (g == k * nw + wid) {
-          pre0[k] = tot0;
-          pre1[k] = tot1;
+      for (int d = 1; d < 32; d <<= 1) {
+        const int ta = __shfl_up_sync(0xffffffffu, va, d);
+        const int tb = __shfl_up_sync(0xffffffffu, vb, d);
+        if (lane >= d) {
+          va += ta;
+          vb += tb;
         }
       }
-      tot0 += sm.gcnt[g];
-      tot1 += sm.gcnt[groups + g];
+      vb += __shfl_sync(0xffffffffu, va, 31);
+      const int tot = __shfl_sync(0xffffffffu, vb, 31);
+      tot0 = tot & 0xffff;
+      tot1 = tot >> 16;
+      const int xa = va - ca, xb = vb - cb;  // exclusive prefixes
+#pragma unroll
+      for (int k = 0; k < kMaxPool; ++k) {
+        const int g = k * nw + wid;  // warp-uniform
+        const int pa = __shfl_sync(0xffffffffu, xa, g & 31);
+        const int pb = __shfl_sync(0xffffffffu, xb, g & 31);
+        const int pre = g < 32 ? pa : pb;
+        pre0[k] = pre & 0xffff;
+        pre1[k] = pre >> 16;
+      }
     }
     if (tot0 + tot1 == 0) break;  // uniform: every thread read the same
     // how many slots of each mode run: all if they fit, else a split in
