@@ -120,23 +120,7 @@ __device__ __forceinline__ bool reg_apply(int (&x)[MAXS], uint32_t d) {
   return ok;
 }
 
-// Propensities (FP32, packed descriptors), their FP64 total, and the
-// direct-method selection for uniform-times-total r, as thread_round.
-template <int MAXR, int MAXS>
-__device__ __forceinline__ double reg_propensities(const ModelView& m,
-                                                   const int (&x)[MAXS],
-                                                   float (&a)[MAXR]) {
-  double a0 = 0.0;
-  auto xget = [&](int i) { return reg_get(x, i); };
-#pragma unroll
-  for (int j = 0; j < MAXR; ++j) {
-    if (j >= m.R) break;
-    a[j] = propensity_packed(m.rate(j), m.pk[j], xget);
-    a0 = __dadd_rn(a0, (double)a[j]);
-  }
-  return a0;
-}
-
+// The direct-method selection for uniform-times-total r, as thread_round.
 template <int MAXR>
 __device__ __forceinline__ int select_reaction(const float (&a)[MAXR], int R,
                                                double r) {
@@ -214,11 +198,12 @@ __host__ __device__ constexpr int spec_lanes(int R, int D) {
 
 // One whole trajectory by the calling warp (all 32 lanes; lane 0 writes).
 // D levels (compile time; the caller checks spec_lanes(R, D) <= 32), at
-// most MAXS species in registers.
-template <int MAXR, int MAXS, int D>
+// most MAXS species in registers; RX: the model's reaction count when the
+// caller fixes it at compile time, else 0.
+template <int MAXR, int MAXS, int D, int RX>
 __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
                               uint64_t traj_id, const TrajOut& o) {
-  const int R = m.R, S = m.S, ita = m.ita, kappa = m.kappa;
+  const int R = RX ? RX : m.R, S = m.S, ita = m.ita, kappa = m.kappa;
   const int lane = threadIdx.x & 31;
   // this lane's depth dl and path j_1 .. j_dl (base-R digits of its index
   // within the depth, first firing first)
@@ -277,24 +262,56 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
     }
   }
 
+  // the reactions' rates and packed descriptors, in registers for the
+  // whole trajectory
+  float rate[MAXR];
+  uint32_t fac[MAXR], net[MAXR];
+#pragma unroll
+  for (int j = 0; j < MAXR; ++j) {
+    rate[j] = j < R ? m.rate(j) : 0.0f;
+    fac[j] = j < R ? m.pk[j] : 0u;
+    net[j] = j < R ? m.pk[R + j] : 0u;
+  }
+  // propensities (FP32, packed descriptors) and their FP64 total, with
+  // thread_round's operations in its order
+  auto props = [&](const int (&xx)[MAXS], float (&a)[MAXR]) {
+    double a0 = 0.0;
+    auto xget = [&](int i) { return reg_get(xx, i); };
+#pragma unroll
+    for (int j = 0; j < MAXR; ++j) {
+      if (j >= R) break;
+      a[j] = propensity_packed(rate[j], fac[j], xget);
+      a0 = __dadd_rn(a0, (double)a[j]);
+    }
+    return a0;
+  };
+  // net change of reaction sel (of reaction 0 for sel < 0)
+  auto net_of = [&](int sel) {
+    uint32_t d = net[0];
+#pragma unroll
+    for (int j = 1; j < MAXR; ++j) d = sel == j ? net[j] : d;
+    return d;
+  };
+  // the firing-sequence hash only when the caller asked for it
+  const bool want_h = o.seqhash != nullptr;
+
   Stream rs = make_stream(ra.seed, traj_id);
   int x[MAXS];
 #pragma unroll
   for (int s = 0; s < MAXS; ++s) x[s] = s < S ? m.x0(s) : 0;
-  // step variates: lane g holds blocks vb + g (cur) and vb + 32 + g (nxt)
+  // step variates: lane g holds blocks vb + g (cur) and vb + 32 + g (nxt).
+  // A pass reads the steps base .. base + D of vb + 32 offsets, base =
+  // steps - vb < 32: offset g (g >= base) from cur of lane g, offset 32 + g
+  // (g < base) from nxt of lane g, so each lane offers the one it owns in
+  // the window (e_w, u_w) and a read is one shuffle.
   uint64_t vb = 0;
-  double e_c, u_c, e_n, u_n;
+  double e_c, u_c, e_n, u_n, e_w, u_w;
   step_variates(rs, (uint64_t)lane, e_c, u_c);
   step_variates(rs, 32u + (uint64_t)lane, e_n, u_n);
   auto variate = [&](int64_t step, double& e, double& u) {
-    const int off = (int)(step - (int64_t)vb);  // 0 <= off < 64
-    const int own = off & 31;
-    const double ec = __shfl_sync(0xffffffffu, e_c, own);
-    const double en = __shfl_sync(0xffffffffu, e_n, own);
-    const double uc = __shfl_sync(0xffffffffu, u_c, own);
-    const double un = __shfl_sync(0xffffffffu, u_n, own);
-    e = off >= 32 ? en : ec;
-    u = off >= 32 ? un : uc;
+    const int own = (int)(step - (int64_t)vb) & 31;
+    e = __shfl_sync(0xffffffffu, e_w, own);
+    u = __shfl_sync(0xffffffffu, u_w, own);
   };
 
   double t = 0.0;
@@ -314,6 +331,11 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
       u_c = u_n;
       step_variates(rs, vb + 32u + (uint64_t)lane, e_n, u_n);
     }
+    {
+      const bool in_cur = lane >= (int)(steps - (int64_t)vb);
+      e_w = in_cur ? e_c : e_n;
+      u_w = in_cur ? u_c : u_n;
+    }
     bool committed = false;
     if (D > 1 && steps + D <= budget) {
       // ---- every lane: the step at the end of its path --------------
@@ -325,7 +347,7 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
         ok &= x[s] + lo[s] >= 0 && x[s] <= (int)PYST_I32MAX - hi[s];
       }
       float a[MAXR];
-      const double a0 = reg_propensities<MAXR>(m, xs, a);
+      const double a0 = props(xs, a);
       double e, u;
       variate(steps + dl, e, u);
       const double tau = __ddiv_rn(e, a0);
@@ -334,7 +356,7 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
       // the state after this lane's step (needed from the deepest lane of
       // the true path, at level D - 1 or D): its range check joins the
       // lane's flag
-      if (dl >= D - 1) ok &= reg_apply(xs, m.pk[R + (sel < 0 ? 0 : sel)]);
+      if (dl >= D - 1) ok &= reg_apply(xs, net_of(sel));
       unsigned sb[kSelBits];
 #pragma unroll
       for (int b = 0; b < kSelBits; ++b)
@@ -387,9 +409,11 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
 #pragma unroll
           for (int s = 0; s < MAXS; ++s)
             x[s] = __shfl_sync(0xffffffffu, xs[s], last);
+          if (want_h) {
 #pragma unroll
-          for (int d = 0; d <= D; ++d)
-            if (d < dn) h = seq_mix(h, (uint64_t)J[d]);
+            for (int d = 0; d <= D; ++d)
+              if (d < dn) h = seq_mix(h, (uint64_t)J[d]);
+          }
           t = tt;
           steps += dn;
           events += dn;
@@ -401,7 +425,7 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
     // ---- D exact single steps ------------------------------------------
     for (int q = 0; q < D && !done; ++q) {
       float a[MAXR];
-      const double a0 = reg_propensities<MAXR>(m, x, a);
+      const double a0 = props(x, a);
       if (a0 == 0.0) {
         status = PYST_TRAJ_ABSORBED;
         fill_state = true;
@@ -432,13 +456,13 @@ __device__ void run_spec_tree(const ModelView& m, const RunArgs& ra,
       }
       t = tn;
       if (done) break;
-      if (!reg_apply(x, m.pk[R + sel])) {
+      if (!reg_apply(x, net_of(sel))) {
         status = PYST_TRAJ_OVERFLOW;
         done = true;
         break;
       }
       events++;
-      h = seq_mix(h, (uint64_t)sel);
+      if (want_h) h = seq_mix(h, (uint64_t)sel);
     }
   }
   if (lane == 0) {
@@ -460,7 +484,7 @@ constexpr int kSpecMaxSpecies = 8;
 // launched only for models whose every reaction packs
 // (blob_reaction_packable) with at most MAXS species.  4 blocks of 128
 // threads per SM: a run of 148 x 16 trajectories is resident at once.
-template <int MAXR, int MAXS, int D>
+template <int MAXR, int MAXS, int D, int RX>
 __global__ void __launch_bounds__(128, 4)
     k_plain_tree(const uint32_t* __restrict__ gblob, int blob_words,
                  int64_t n_traj, uint64_t id_base, RunArgs ra, OutBase ob) {
@@ -492,15 +516,15 @@ __global__ void __launch_bounds__(128, 4)
   m.fast = __syncthreads_and(pack_reactions(m, pk)) != 0;
   for (; u < n_traj; u += nwarps) {
     const TrajOut o = ob.at(0, u, 0, 0, ob.stride, m.R);
-    run_spec_tree<MAXR, MAXS, D>(m, ra, id_base + (uint64_t)u, o);
+    run_spec_tree<MAXR, MAXS, D, RX>(m, ra, id_base + (uint64_t)u, o);
   }
 }
 
-template <int MAXR, int MAXS, int D>
+template <int MAXR, int MAXS, int D, int RX>
 int launch_tree(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
                 uint64_t id_base, const RunArgs& ra, const OutBase& ob,
                 cudaStream_t st) {
-  auto kf = k_plain_tree<MAXR, MAXS, D>;
+  auto kf = k_plain_tree<MAXR, MAXS, D, RX>;
   const size_t smem = (size_t)mi.words * 4 + 16 + packed_bytes(mi.R);
   const int rc = set_smem(kf, smem);
   if (rc) return rc;
@@ -511,19 +535,37 @@ int launch_tree(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
 }
 
 // The lane tree for a packable model of at most 8 reactions and
-// kSpecMaxSpecies species: depth 5 for R <= 2, 3 for R <= 4, 2 for R <= 8.
+// kSpecMaxSpecies species: depth 5 for R <= 2, 3 for R <= 4, 2 for R <= 8;
+// the reaction count fixed at compile time for R = 2, 3, 4, the species
+// registers sized 2, 4 or 8.
+template <int MAXS>
+int launch_tree_s(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
+                  uint64_t id_base, const RunArgs& ra, const OutBase& ob,
+                  cudaStream_t st) {
+  switch (mi.R) {
+    case 2:
+      return launch_tree<2, MAXS, 5, 2>(d_blob, mi, n, id_base, ra, ob, st);
+    case 3:
+      return launch_tree<3, MAXS, 3, 3>(d_blob, mi, n, id_base, ra, ob, st);
+    case 4:
+      return launch_tree<4, MAXS, 3, 4>(d_blob, mi, n, id_base, ra, ob, st);
+    default:
+      return mi.R < 2
+                 ? launch_tree<2, MAXS, 5, 0>(d_blob, mi, n, id_base, ra, ob,
+                                              st)
+                 : launch_tree<8, MAXS, 2, 0>(d_blob, mi, n, id_base, ra, ob,
+                                              st);
+  }
+}
+
 int launch_tree_for(const uint32_t* d_blob, const HostModelInfo& mi,
                     int64_t n, uint64_t id_base, const RunArgs& ra,
                     const OutBase& ob, cudaStream_t st) {
-  const bool s4 = mi.S <= 4;
-  if (mi.R <= 2)
-    return s4 ? launch_tree<4, 4, 5>(d_blob, mi, n, id_base, ra, ob, st)
-              : launch_tree<4, 8, 5>(d_blob, mi, n, id_base, ra, ob, st);
-  if (mi.R <= 4)
-    return s4 ? launch_tree<4, 4, 3>(d_blob, mi, n, id_base, ra, ob, st)
-              : launch_tree<4, 8, 3>(d_blob, mi, n, id_base, ra, ob, st);
-  return s4 ? launch_tree<8, 4, 2>(d_blob, mi, n, id_base, ra, ob, st)
-            : launch_tree<8, 8, 2>(d_blob, mi, n, id_base, ra, ob, st);
+  if (mi.S <= 2)
+    return launch_tree_s<2>(d_blob, mi, n, id_base, ra, ob, st);
+  if (mi.S <= 4)
+    return launch_tree_s<4>(d_blob, mi, n, id_base, ra, ob, st);
+  return launch_tree_s<8>(d_blob, mi, n, id_base, ra, ob, st);
 }
 
 template <int MAXR, int LG>

@@ -404,7 +404,8 @@ def test_small_runs_at_the_packing_boundary(torch_cuda, built_lib,
     sides of the packed-descriptor limits: the host picks the lane tree for
     packable ones and the lockstep lane groups otherwise; both equal the
     oracle.  Also every lane-tree depth: R = 1 and 2 (5 levels), 3 and 4
-    (3 levels), 5 to 8 (2 levels)."""
+    (3 levels), 5 to 8 (2 levels), each with 2, 4 and 8 species registers
+    (S = 2, 3-4, 5-8)."""
     from py_stoch_b200 import _lib
     t = np.linspace(0, 0.05, 6).astype(np.float32)
     models = []
@@ -416,10 +417,11 @@ def test_small_runs_at_the_packing_boundary(torch_cuda, built_lib,
                                         [1e-3], [60, 0], t))
     models.append(Model.mass_action([[1], [1], [1]], [[0], [0], [2]], [1.0],
                                     [90, 90, 90], t))
-    for R in (1, 2, 5, 8):
-        models += networks.synthetic_networks(1, seed=40 + R, s_range=(2, 6),
-                                              r_range=(R, R),
-                                              t_range=(0.002, 0.01))
+    for R in (1, 2, 3, 4, 5, 8):
+        for k, sr in enumerate(((2, 2), (3, 4), (5, 8))):
+            models += networks.synthetic_networks(
+                1, seed=40 + 3 * R + k, s_range=sr, r_range=(R, R),
+                t_range=(0.002, 0.01))
     kinds = set()
     for i, m in enumerate(models):
         kinds.add(built_lib.pyst_test_model_packable(m.blob().ctypes.data))
