@@ -33,16 +33,20 @@ namespace {
 
 // Round lengths of the mode-sorted tau-leaping kernel: SSA steps and leaps
 // a trajectory advances between two regroupings of its block.  On the
-// Schlogl workload (262144 trajectories, 896-thread blocks) 32 / 3 measured
-// 81.0 ms a step, 24 / 2 81.6, 32 / 2 82.8, 48 / 3 83.0; with 1024-thread
-// blocks longer rounds were slower still (128 / 8 100, 256 / 16 107,
-// 256 / 32 121), and resizing leap rounds to match the SSA rounds'
-// measured time was slower too.
+// Schlogl workload (262144 trajectories, 896-thread blocks, SSA fallback
+// rounds of 100 steps) 40 / 4 measured 64.3 ms a step, 20 / 2 64.5,
+// 50 / 5 64.6, 40 / 3 65.7, 60 / 6 66.1, 30 / 3 66.6, 32 / 3 68.3, 36 / 4
+// 69.2, 48 / 4 69.1, 45 / 4 70.0, 10 / 1 71.1 (a comb in the SSA length:
+// where the fallback's 100th step, and with it the DECIDE that may switch
+// the trajectory out of its SSA warp, falls within a round sets how long
+// lanes idle); with 1024-thread blocks longer rounds were slower still
+// (128 / 8 100, 256 / 16 107, 256 / 32 121, earlier kernels), and resizing
+// leap rounds to match the SSA rounds' measured time was slower too.
 #ifndef PYST_CAP_SSA
-#define PYST_CAP_SSA 32
+#define PYST_CAP_SSA 40
 #endif
 #ifndef PYST_CAP_LEAP
-#define PYST_CAP_LEAP 3
+#define PYST_CAP_LEAP 4
 #endif
 constexpr int kSortedCapSsa = PYST_CAP_SSA;
 // Auto mapping of networks with more reactions than the register engine:

@@ -590,16 +590,32 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
         bool ok = false;
         while (true) {
           bool bad = false;
+          auto draw = [&](int j, float aj) {
+            if ((crit >> j) & 1u) return (j == kcrit) ? 1 : 0;
+            const float lam = __fmul_rn(aj, (float)tau);
+            const int k = poisson(lam, leap_key(rs, leap_q, j, retry));
+            if (k < 0) bad = true;
+            return k < 0 ? 0 : k;
+          };
+          if constexpr (GROUP != kGroupAny) {
+            // (the mode-sorted scheduler's leap rounds) one reaction per
+            // iteration, not unrolled: a single inlined copy of the
+            // sampler's call sequence, a[j] and K[j] by unrolled selects
+#pragma unroll 1
+            for (int j = 0; j < R; ++j) {
+              float aj = a[0];
 #pragma unroll
-          for (int j = 0; j < MAXR; ++j) {
-            if (j >= R) break;
-            if ((crit >> j) & 1u) {
-              K[j] = (j == kcrit) ? 1 : 0;
-            } else {
-              const float lam = __fmul_rn(a[j], (float)tau);
-              const int k = poisson(lam, leap_key(rs, leap_q, j, retry));
-              if (k < 0) bad = true;
-              K[j] = k < 0 ? 0 : k;
+              for (int q = 1; q < MAXR; ++q) aj = (j == q) ? a[q] : aj;
+              const int kj = draw(j, aj);
+#pragma unroll
+              for (int q = 0; q < MAXR; ++q)
+                if (q == j) K[q] = kj;
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < MAXR; ++j) {
+              if (j >= R) break;
+              K[j] = draw(j, a[j]);
             }
           }
           if (bad) {
