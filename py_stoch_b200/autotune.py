@@ -33,7 +33,7 @@ N_EDGES = (4096, 65536, 1 << 20, 1 << 40)
 # Candidate geometries of the mode-sorted scheduler: (SSA steps, leaps) per
 # round x slots per thread x block size.  Every one gives the same results
 # (the schedule never changes a trajectory's arithmetic).
-ROUNDS = ((16, 2), (20, 2), (32, 3), (40, 4), (64, 4))
+ROUNDS = ((16, 2), (20, 2), (32, 3), (40, 4), (50, 5), (64, 4))
 POOLS = (1, 2)
 SORTED_BLOCKS = (896, 448)
 

@@ -445,7 +445,13 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
   auto xget = [&](int i) { return XV(i); };
 
   while (true) {
-    if (n_ssa >= cap_ssa || n_leap >= cap_leap) break;
+    // an SSA-group round whose cap falls where a DECIDE is due runs the
+    // DECIDE before stopping, so the slot's next round is in the group of
+    // its outcome (it would otherwise spend that round only switching).
+    // (Leap-group rounds do not: their slots would run every continuing
+    // leap's DECIDE twice.)
+    const bool capped = n_ssa >= cap_ssa || n_leap >= cap_leap;
+    if (capped && !(GROUP == kGroupSsa && !ssa_mode)) break;
     float a[MAXR];
     double a0 = 0.0;
 #pragma unroll
@@ -542,11 +548,13 @@ __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
         ssa_left = ra.ssa_fallback_steps;
         leap_grp = false;
         // regroup before stepping
-        if (GROUP == kGroupLeap || (stop_on_switch && group_leap)) break;
+        if (capped || GROUP == kGroupLeap || (stop_on_switch && group_leap))
+          break;
         // fall through to the SSA step below with the same propensities
       } else {
         leap_grp = true;
-        if (GROUP == kGroupSsa || (stop_on_switch && !group_leap)) break;
+        if (capped || GROUP == kGroupSsa || (stop_on_switch && !group_leap))
+          break;
         // ---------------- leap ---------------------------------------
         steps++;
         n_leap++;
