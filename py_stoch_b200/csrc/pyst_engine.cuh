@@ -382,14 +382,17 @@ __device__ __forceinline__ void thread_init(const ModelView& m, int32_t* xcol,
 // steps) -- the same arithmetic, a smaller instruction footprint per warp.
 enum { kPkLists = 0, kPkPacked = 1, kPkRuntime = 2 };
 enum { kGroupAny = 0, kGroupSsa = 1, kGroupLeap = 2 };
+// RX: the model's reaction count when the caller fixes it at compile time
+// (the per-reaction loops then carry no run-time bound), else 0.
 template <int MAXR, bool TAU, bool SCORE, int PK, int LG = 1,
-          int GROUP = kGroupAny>
+          int GROUP = kGroupAny, int RX = 0>
 __device__ void thread_round(const ModelView& m, int32_t* xcol, int64_t* slot,
                              int bs, int ss, const RunArgs& ra,
                              uint64_t traj_id, TState& st, double* integ,
                              int* cnt, const TrajOut& o, int cap_ssa,
                              int cap_leap, bool stop_on_switch) {
-  const int S = m.S, R = m.R, ita = m.ita, kappa = m.kappa;
+  static_assert(RX == 0 || RX == MAXR, "an exact reaction count is MAXR");
+  const int S = m.S, R = RX ? RX : m.R, ita = m.ita, kappa = m.kappa;
   const bool pk = PK == kPkPacked || (PK == kPkRuntime && m.fast);
   // general kinetic laws: entry-list form only (a model with laws never
   // packs, and the sorted kernel's run-time form is not given such models)
@@ -857,7 +860,8 @@ __device__ void thread_finish(const ModelView& m, const int32_t* xcol, int bs,
 // One whole trajectory by the calling thread.  PK: kPkPacked or kPkLists
 // when the caller knows the form (the host checks packability), -1 to
 // choose by m.fast at run time (batched launches mix models).
-template <int MAXR, bool TAU, bool SCORE, int PK = -1>
+// RX as thread_round's.
+template <int MAXR, bool TAU, bool SCORE, int PK = -1, int RX = 0>
 __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
                            int bs, const RunArgs& ra, uint64_t traj_id,
                            const TrajOut& o) {
@@ -871,13 +875,13 @@ __device__ void run_thread(const ModelView& m, int32_t* xcol, int64_t* slot,
     cnt[j] = 0;
   }
   if (PK == kPkPacked || (PK < 0 && m.fast))
-    thread_round<MAXR, TAU, SCORE, kPkPacked>(m, xcol, slot, bs, bs, ra,
-                                              traj_id, st, integ, cnt, o,
-                                              0x7fffffff, 0x7fffffff, false);
+    thread_round<MAXR, TAU, SCORE, kPkPacked, 1, kGroupAny, RX>(
+        m, xcol, slot, bs, bs, ra, traj_id, st, integ, cnt, o, 0x7fffffff,
+        0x7fffffff, false);
   else if (PK == kPkLists || PK < 0)
-    thread_round<MAXR, TAU, SCORE, kPkLists>(m, xcol, slot, bs, bs, ra,
-                                             traj_id, st, integ, cnt, o,
-                                             0x7fffffff, 0x7fffffff, false);
+    thread_round<MAXR, TAU, SCORE, kPkLists, 1, kGroupAny, RX>(
+        m, xcol, slot, bs, bs, ra, traj_id, st, integ, cnt, o, 0x7fffffff,
+        0x7fffffff, false);
   thread_finish<MAXR, SCORE>(m, xcol, bs, st, integ, cnt, o);
 }
 
@@ -1167,10 +1171,10 @@ __device__ void thread_round_big(const ModelView& m, int32_t* xcol,
 #undef SL
 }
 
-// thread_round for MAXR > 0 (register arrays), thread_round_big for 0; PK
-// and GROUP as thread_round's
+// thread_round for MAXR > 0 (register arrays), thread_round_big for 0; PK,
+// GROUP and RX as thread_round's
 template <int MAXR, bool TAU, bool SCORE, int PK = kPkRuntime,
-          int GROUP = kGroupAny>
+          int GROUP = kGroupAny, int RX = 0>
 __device__ __forceinline__ void any_round(
     const ModelView& m, int32_t* xcol, int64_t* slot, int bs, int ss,
     const RunArgs& ra, uint64_t traj_id, TState& st, double* integ, int* cnt,
@@ -1180,10 +1184,9 @@ __device__ __forceinline__ void any_round(
     thread_round_big<TAU>(m, xcol, slot, bs, ss, ra, traj_id, st, o, cap_ssa,
                           cap_leap, stop_on_switch);
   } else {
-    thread_round<MAXR, TAU, SCORE, PK, 1, GROUP>(m, xcol, slot, bs, ss, ra,
-                                                 traj_id, st, integ, cnt, o,
-                                                 cap_ssa, cap_leap,
-                                                 stop_on_switch);
+    thread_round<MAXR, TAU, SCORE, PK, 1, GROUP, RX>(
+        m, xcol, slot, bs, ss, ra, traj_id, st, integ, cnt, o, cap_ssa,
+        cap_leap, stop_on_switch);
   }
 }
 

@@ -28,9 +28,11 @@ namespace PYST_CAT(thread_flavour_, PYST_TAU, PYST_SCORE) {
 #endif
 
 
+
 // PK: kPkPacked for models whose every reaction packs (the host checks),
-// kPkLists otherwise (general kinetic laws included).
-template <int MAXR, bool TAU, bool SCORE, int PK>
+// kPkLists otherwise (general kinetic laws included).  RX: MAXR when the
+// model has exactly MAXR reactions (the host checks), else 0.
+template <int MAXR, bool TAU, bool SCORE, int PK, int RX = 0>
 __global__ void __launch_bounds__(128, PYST_THREAD_MINB)
     k_plain_thread(const uint32_t* __restrict__ gblob, int blob_words,
                    int64_t n_traj, uint64_t id_base, RunArgs ra, OutBase ob,
@@ -77,7 +79,7 @@ __global__ void __launch_bounds__(128, PYST_THREAD_MINB)
     if constexpr (MAXR == 0)
       run_thread_big<TAU>(m, xcol, slot, bs, ra, id_base + (uint64_t)u, o);
     else
-      run_thread<MAXR, TAU, SCORE, PK>(m, xcol, slot, bs, ra,
+      run_thread<MAXR, TAU, SCORE, PK, RX>(m, xcol, slot, bs, ra,
                                        id_base + (uint64_t)u, o);
     u = nthreads + (int64_t)atomicAdd(queue, 1ull);
   }
@@ -633,16 +635,10 @@ int launch_group(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
 }
 #endif
 
-template <int MR>
-int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
-               uint64_t id_base, const RunArgs& ra, const OutBase& ob, int bs,
-               cudaStream_t st, size_t smem, unsigned long long* queue) {
-  // the packed-descriptor form compiled on its own for packable models
-  auto kf = (MR > 0 && mi.packable)
-                ? k_plain_thread<MR, (bool)PYST_TAU, (bool)PYST_SCORE,
-                                 kPkPacked>
-                : k_plain_thread<MR, (bool)PYST_TAU, (bool)PYST_SCORE,
-                                 kPkLists>;
+template <class K>
+int launch_k(K kf, const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
+             uint64_t id_base, const RunArgs& ra, const OutBase& ob, int bs,
+             cudaStream_t st, size_t smem, unsigned long long* queue) {
   const int rc = set_smem(kf, smem);
   if (rc) return rc;
   int per_sm = 1;
@@ -654,6 +650,55 @@ int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
   kf<<<(unsigned)grid, bs, smem, st>>>(d_blob, mi.words, n, id_base, ra, ob,
                                        queue);
   return cudaGetLastError() == cudaSuccess ? PYST_OK : PYST_ECUDA;
+}
+
+template <int MR>
+int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
+               uint64_t id_base, const RunArgs& ra, const OutBase& ob, int bs,
+               cudaStream_t st, size_t smem, unsigned long long* queue) {
+  // the packed-descriptor form compiled on its own for packable models
+  auto kf = (MR > 0 && mi.packable)
+                ? k_plain_thread<MR, (bool)PYST_TAU, (bool)PYST_SCORE,
+                                 kPkPacked>
+                : k_plain_thread<MR, (bool)PYST_TAU, (bool)PYST_SCORE,
+                                 kPkLists>;
+  return launch_k(kf, d_blob, mi, n, id_base, ra, ob, bs, st, smem, queue);
+}
+
+// A packable model of 2 to 8 reactions: the packed form with the reaction
+// count fixed at compile time (its per-reaction loops carry no run-time
+// bound): telegraph gradient forward, 1M trajectories, 208.5 -> 173.6 ms;
+// Schlogl direct method, 262144 trajectories, 170 -> 152.5 ms.
+template <int RXV>
+int launch_exact(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
+                 uint64_t id_base, const RunArgs& ra, const OutBase& ob,
+                 int bs, cudaStream_t st, size_t smem,
+                 unsigned long long* queue) {
+  return launch_k(
+      k_plain_thread<RXV, (bool)PYST_TAU, (bool)PYST_SCORE, kPkPacked, RXV>,
+      d_blob, mi, n, id_base, ra, ob, bs, st, smem, queue);
+}
+
+int launch_exact_r(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
+                   uint64_t id_base, const RunArgs& ra, const OutBase& ob,
+                   int bs, cudaStream_t st, size_t smem,
+                   unsigned long long* queue) {
+  switch (mi.R) {
+#define PYST_EXACT_CASE(r)                                                  \
+  case r:                                                                   \
+    return launch_exact<r>(d_blob, mi, n, id_base, ra, ob, bs, st, smem,    \
+                           queue);
+    PYST_EXACT_CASE(2)
+    PYST_EXACT_CASE(3)
+    PYST_EXACT_CASE(4)
+    PYST_EXACT_CASE(5)
+    PYST_EXACT_CASE(6)
+    PYST_EXACT_CASE(7)
+    PYST_EXACT_CASE(8)
+#undef PYST_EXACT_CASE
+    default:
+      return PYST_EUNSUPPORTED;
+  }
 }
 
 }  // namespace (flavour)
@@ -692,6 +737,9 @@ int PYST_CAT(launch_plain_thread_, PYST_TAU, PYST_SCORE)(
     return launch_group<8>(d_blob, mi, n, id_base, ra, ob, bs, st, smem);
   }
 #endif
+  if (mi.packable && mi.R >= 2 && mi.R <= 8)
+    return launch_exact_r(d_blob, mi, n, id_base, ra, ob, bs, st, smem,
+                          queue);
   if (maxr <= 4)
     return launch_one<4>(d_blob, mi, n, id_base, ra, ob, bs, st, smem, queue);
   if (maxr <= 8)

@@ -431,3 +431,34 @@ def test_small_runs_at_the_packing_boundary(torch_cuda, built_lib,
                     step_budget=200000)
         _compare(g, o)
     assert kinds == {0, 1}
+
+
+@pytest.mark.parametrize('R', [2, 3, 4, 5, 6, 7, 8, 16, 32])
+def test_exact_reaction_counts(torch_cuda, built_lib, oracle_mod, R):
+    """Packable models with 2 to 8 reactions run thread-mapped kernels with
+    the reaction count fixed at compile time (the direct method and the
+    simple tau loop, with and without scores), and the mode-sorted kernel
+    does so when R equals its register-array size (4, 8, 16, 32): each
+    equals the oracle.  2,500 trajectories put the direct method above the
+    small-run limit of the lane tree."""
+    # seeds whose networks take both SSA steps and leaps (oracle, 100
+    # trajectories: 150-520 leaps and 1,200-1,800 SSA steps each)
+    seed = {2: 69, 3: 76, 4: 78, 5: 66, 6: 70, 7: 69, 8: 71, 16: 106,
+            32: 123}[R]
+    m = networks.synthetic_networks(1, seed=seed, s_range=(3, 8),
+                                    r_range=(R, R), t_range=(0.002, 0.02),
+                                    x0_max=100000, k_range=(1e-5, 1e1))[0]
+    n = 2500
+    for method, kw in (('direct', {}), ('tau', {}),
+                       ('tau', {'sorted_blocks': False})):
+        g = _gpu(torch_cuda, m, n, method, 'thread', seed=R,
+                 step_budget=100000, **kw)
+        o = _oracle(oracle_mod, m, n, method, 'thread', seed=R,
+                    step_budget=100000)
+        _compare(g, o)
+    if R <= 8:
+        g = _gpu(torch_cuda, m, n, 'direct', 'thread', seed=R + 1,
+                 step_budget=100000, score=True)
+        o = _oracle(oracle_mod, m, n, 'direct', 'thread', seed=R + 1,
+                    step_budget=100000)
+        _compare(g, o, score=True)
