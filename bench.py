@@ -50,8 +50,8 @@ def workloads():
             # from one ncu capture of the simulation kernel on 229,376
             # trajectories: DRAM read + write per trajectory, and warp
             # instructions per reaction event
-            dram_bytes_per_traj=(471.92e6 + 1070.73e6) / 229376,
-            warp_inst_per_event=35214719170 / 4209068063),
+            dram_bytes_per_traj=(462.53e6 + 1004.32e6) / 229376,
+            warp_inst_per_event=33041358745 / 4209068063),
         'lv_ssa': dict(
             model=networks.lotka_volterra(), n=1024, method='direct',
             desc='plain Gillespie direct method, Lotka-Volterra (k1=10, '
