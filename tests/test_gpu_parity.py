@@ -462,3 +462,33 @@ def test_exact_reaction_counts(torch_cuda, built_lib, oracle_mod, R):
         o = _oracle(oracle_mod, m, n, 'direct', 'thread', seed=R + 1,
                     step_budget=100000)
         _compare(g, o, score=True)
+
+
+def test_batch_exact_reaction_counts(torch_cuda, built_lib, oracle_mod):
+    """Batched thread-mapped items of 2 to 8 reactions run with the reaction
+    count fixed at compile time; each item equals the oracle (tau-leaping
+    and the direct method, with scores)."""
+    from py_stoch_b200.batch import Batch
+    seeds = {2: 69, 3: 76, 4: 78, 5: 66, 6: 70, 7: 69, 8: 71}
+    models = [networks.synthetic_networks(
+        1, seed=s, s_range=(3, 8), r_range=(R, R), t_range=(0.002, 0.02),
+        x0_max=100000, k_range=(1e-5, 1e1))[0] for R, s in seeds.items()]
+    n, budget = 96, 100000
+    for method in ('tau', 'direct'):
+        b = Batch(models, n, method=method, mapping='thread', score=True,
+                  small_batch_warps=False)
+        b.run(seed=5, step_budget=budget)
+        torch_cuda.cuda.synchronize()
+        for i, m in enumerate(models):
+            o = oracle_mod.simulate(m, n, 1 if method == 'tau' else 0,
+                                    seed=5,
+                                    traj_id_base=int(b.traj_id_base[i]),
+                                    step_budget=budget)
+            np.testing.assert_array_equal(b.samples(i).cpu().numpy(),
+                                          o['samples'])
+            np.testing.assert_array_equal(
+                b.per_traj('status', i).cpu().numpy(), o['status'])
+            np.testing.assert_array_equal(
+                b.per_traj('events', i).cpu().numpy(), o['events'])
+            np.testing.assert_allclose(b.score(i).cpu().numpy(), o['score'],
+                                       rtol=T_RTOL, atol=1e-12)
