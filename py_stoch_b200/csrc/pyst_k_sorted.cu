@@ -423,6 +423,16 @@ int launch_one(const uint32_t* d_blob, const HostModelInfo& mi, int64_t n,
   // reaction count fixed at compile time (Schlogl, R = 4: 64.0 -> 57.8 ms)
   if (MR > 0 && mi.packable && block == kMaxBlock && mi.R == MR)
     kf = k_tau_sorted<MR, kMaxBlock, kPk, MR>;
+  // and the reaction counts between (2, 3 and 5 to 7), without scores
+  if constexpr (!kScore && (MR == 4 || MR == 8)) {
+    if (mi.packable && block == kMaxBlock) {
+      if (MR == 4 && mi.R == 2) kf = k_tau_sorted<2, kMaxBlock, kPkPacked, 2>;
+      if (MR == 4 && mi.R == 3) kf = k_tau_sorted<3, kMaxBlock, kPkPacked, 3>;
+      if (MR == 8 && mi.R == 5) kf = k_tau_sorted<5, kMaxBlock, kPkPacked, 5>;
+      if (MR == 8 && mi.R == 6) kf = k_tau_sorted<6, kMaxBlock, kPkPacked, 6>;
+      if (MR == 8 && mi.R == 7) kf = k_tau_sorted<7, kMaxBlock, kPkPacked, 7>;
+    }
+  }
   const int rc = set_smem(kf, smem);
   if (rc) return rc;
   if (cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st) !=
