@@ -457,11 +457,14 @@ def test_exact_reaction_counts(torch_cuda, built_lib, oracle_mod, R):
                     step_budget=100000)
         _compare(g, o)
     if R <= 8:
-        g = _gpu(torch_cuda, m, n, 'direct', 'thread', seed=R + 1,
-                 step_budget=100000, score=True)
-        o = _oracle(oracle_mod, m, n, 'direct', 'thread', seed=R + 1,
-                    step_budget=100000)
-        _compare(g, o, score=True)
+        # with scores: the direct method's exact-R kernels, and the sorted
+        # kernel's score flavour (exact R for R = 4 and 8)
+        for method in ('direct', 'tau'):
+            g = _gpu(torch_cuda, m, n, method, 'thread', seed=R + 1,
+                     step_budget=100000, score=True)
+            o = _oracle(oracle_mod, m, n, method, 'thread', seed=R + 1,
+                        step_budget=100000)
+            _compare(g, o, score=True)
 
 
 def test_batch_exact_reaction_counts(torch_cuda, built_lib, oracle_mod):
