@@ -50,8 +50,8 @@ def workloads():
             # from one ncu capture of the simulation kernel on 229,376
             # trajectories: DRAM read + write per trajectory, and warp
             # instructions per reaction event
-            dram_bytes_per_traj=(462.53e6 + 1004.32e6) / 229376,
-            warp_inst_per_event=33041358745 / 4209068063),
+            dram_bytes_per_traj=(466.38e6 + 1003.97e6) / 229376,
+            warp_inst_per_event=32554582830 / 4209068063),
         'lv_ssa': dict(
             model=networks.lotka_volterra(), n=1024, method='direct',
             desc='plain Gillespie direct method, Lotka-Volterra (k1=10, '
